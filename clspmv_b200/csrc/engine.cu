@@ -1,0 +1,738 @@
+// Device engine of the Cocktail SpMV: uploads every sub-matrix of a cocktail,
+// selects one kernel per sub-matrix and launches them into one accumulated
+// result, the role of clSpMV_NV/src/spmv_cocktail.cpp (init_mat_kernels :1593,
+// do_spmv :1091, the cpy_* functions :1462-1591, free_mat_kernels :1616).
+//
+// Launch order per SpMV is the reference's (do_spmv :1091-1135): BDIA, DIA,
+// SBELL, BELL, BCSR, SELL, ELL, CSR, COO (segment pass + fix-up pass).  Every
+// kernel reads x and read-modify-writes y on one stream, so the parts compose
+// without synchronisation; with CSP_FLAG_GRAPH the whole sequence is one CUDA
+// graph replayed per SpMV.
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <algorithm>
+#include <cmath>
+#include <string>
+#include <vector>
+
+#include "csp/clspmv.h"
+#include "internal.h"
+#include "engine.h"
+#include "kernels/flat.cuh"
+#include "kernels/diag.cuh"
+#include "kernels/block.cuh"
+
+namespace csp {
+
+static thread_local std::string g_last_error;
+
+int set_error(int code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+void clear_error() { g_last_error.clear(); }
+
+int cuda_error(cudaError_t e, const char* what)
+{
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+        return set_error(CSP_ENODEV, "%s: %s", what, cudaGetErrorString(e));
+    if (e == cudaErrorMemoryAllocation) return set_error(CSP_ENOMEM, "%s: %s", what, cudaGetErrorString(e));
+    return set_error(CSP_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CSP_CUDA(call)                                              \
+    do {                                                            \
+        cudaError_t _e = (call);                                    \
+        if (_e != cudaSuccess) return cuda_error(_e, #call);        \
+    } while (0)
+
+// --------------------------------------------------------------------------
+// device memory
+// --------------------------------------------------------------------------
+int Engine::alloc(void** p, size_t bytes)
+{
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMalloc");
+    allocations.push_back(*p);
+    device_bytes += bytes;
+    return CSP_OK;
+}
+
+// Copies n host ints to a new device array of at least `cap` entries (zero tail).
+int Engine::upload_int(int** d, const int* h, size_t n, size_t cap)
+{
+    cap = std::max(cap, n);
+    int rc = alloc(reinterpret_cast<void**>(d), cap * sizeof(int));
+    if (rc) return rc;
+    if (cap > n) CSP_CUDA(cudaMemset(*d + n, 0, (cap - n) * sizeof(int)));
+    if (n) CSP_CUDA(cudaMemcpy(*d, h, n * sizeof(int), cudaMemcpyHostToDevice));
+    return CSP_OK;
+}
+
+// Round-to-nearest-even FP32 -> BF16 (NaN kept quiet).
+static inline uint16_t to_bf16(float f)
+{
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40);
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
+
+// Matrix values in the handle's storage type (FP32, or BF16 with CSP_FLAG_BF16).
+int Engine::upload_val(void** d, const float* h, size_t n, size_t cap)
+{
+    cap = std::max(cap, n);
+    const size_t es = bf16 ? 2 : 4;
+    int rc = alloc(d, cap * es);
+    if (rc) return rc;
+    if (cap > n) CSP_CUDA(cudaMemset(static_cast<char*>(*d) + n * es, 0, (cap - n) * es));
+    if (!n) return CSP_OK;
+    if (!bf16) {
+        CSP_CUDA(cudaMemcpy(*d, h, n * 4, cudaMemcpyHostToDevice));
+    } else {
+        std::vector<uint16_t> t(n);
+        for (size_t i = 0; i < n; i++) t[i] = to_bf16(h[i]);
+        CSP_CUDA(cudaMemcpy(*d, t.data(), n * 2, cudaMemcpyHostToDevice));
+    }
+    return CSP_OK;
+}
+
+Engine::~Engine()
+{
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    for (void* p : allocations) cudaFree(p);
+    if (own_stream) cudaStreamDestroy(own_stream);
+}
+
+static inline int pad_to(int v, int a) { return (v + a - 1) / a * a; }
+static inline unsigned grid_for(long long threads, int block) { return (unsigned)((threads + block - 1) / block); }
+
+// --------------------------------------------------------------------------
+// Per-format setup.  Each validates the struct, uploads it and fixes the launch.
+// --------------------------------------------------------------------------
+int Engine::add_csr(const csr_matrix_if& c, int method)
+{
+    const int m = c.matinfo.height;
+    if (m < 0 || !c.csr_row_ptr) return set_error(CSP_EINVAL, "CSR part: bad row pointer");
+    const int nnz = c.csr_row_ptr[m];
+    if (nnz < 0 || (nnz > 0 && (!c.csr_col_id || !c.csr_data))) return set_error(CSP_EINVAL, "CSR part: bad arrays");
+    if (m > height) return set_error(CSP_EINVAL, "CSR part taller than the cocktail");
+    Part p;
+    p.kind = PART_CSR;
+    p.method = method;
+    p.m = m;
+    p.nnz = nnz;
+    int rc;
+    if (method == 6) {
+        // float4 scalar kernel on the row-padded CSR (util.cpp:31 pad_csr with 4)
+        csr_matrix_if padded;
+        csp_init_csr_matrix(&padded);
+        rc = csp_pad_csr(&c, &padded, 4);
+        if (rc) { csp_free_csr_matrix(&padded); return rc; }
+        const int pn = padded.matinfo.nnz;
+        if ((rc = upload_int(&p.i0, padded.csr_row_ptr, (size_t)m + 1, (size_t)m + 1)) ||
+            (rc = upload_int(&p.i1, padded.csr_col_id, pn, (size_t)pad_to(pn, 4) + 4)) ||
+            (rc = upload_val(&p.v, padded.csr_data, pn, (size_t)pad_to(pn, 4) + 4))) {
+            csp_free_csr_matrix(&padded);
+            return rc;
+        }
+        csp_free_csr_matrix(&padded);
+    } else {
+        if ((rc = upload_int(&p.i0, c.csr_row_ptr, (size_t)m + 1, (size_t)m + 1)) ||
+            (rc = upload_int(&p.i1, c.csr_col_id, nnz, (size_t)pad_to(nnz, 4) + 4)) ||
+            (rc = upload_val(&p.v, c.csr_data, nnz, (size_t)pad_to(nnz, 4) + 4)))
+            return rc;
+    }
+    if (method == 2) {
+        // row blocks: <= kAdaptNnz entries and <= kAdaptThreads rows, or one long row
+        std::vector<int> blocks;
+        blocks.push_back(0);
+        int r = 0;
+        while (r < m) {
+            const int start = r;
+            long long acc = 0;
+            while (r < m && r - start < dev::kAdaptThreads) {
+                const int len = c.csr_row_ptr[r + 1] - c.csr_row_ptr[r];
+                if (acc + len > dev::kAdaptNnz) break;
+                acc += len;
+                r++;
+            }
+            if (r == start) r++;   // a row longer than the budget forms its own block
+            blocks.push_back(r);
+        }
+        p.nblocks = (int)blocks.size() - 1;
+        if ((rc = upload_int(&p.i2, blocks.data(), blocks.size(), blocks.size()))) return rc;
+    }
+    if (method == 3) {
+        const double mean = m ? (double)nnz / m : 0.0;
+        int g = 2;
+        while (g < 32 && g * 2 <= mean) g *= 2;  // ~ one 4-wide vector per lane per row
+        p.group = g;
+    }
+    parts.push_back(p);
+    return CSP_OK;
+}
+
+int Engine::add_coo(const coo_matrix_if& c)
+{
+    const int nnz = c.matinfo.nnz;
+    if (nnz < 0 || (nnz > 0 && (!c.coo_row_id || !c.coo_col_id || !c.coo_data)))
+        return set_error(CSP_EINVAL, "COO part: bad arrays");
+    if (nnz == 0) return CSP_OK;
+    for (int i = 0; i + 1 < nnz; i++)
+        if (c.coo_row_id[i] > c.coo_row_id[i + 1]) return set_error(CSP_EINVAL, "COO part: rows not sorted");
+    for (int i = 0; i < nnz; i++)
+        if (c.coo_row_id[i] < 0 || c.coo_row_id[i] >= height || c.coo_col_id[i] < 0 || c.coo_col_id[i] >= width)
+            return set_error(CSP_EINVAL, "COO part: entry %d out of range", i);
+    Part p;
+    p.kind = PART_COO;
+    p.method = 0;
+    p.nnz = nnz;
+    // pad to whole 128-entry tiles with (last row, last col, 0.0)
+    const int npad = pad_to(nnz, 128);
+    std::vector<int> r(c.coo_row_id, c.coo_row_id + nnz), cl(c.coo_col_id, c.coo_col_id + nnz);
+    std::vector<float> v(c.coo_data, c.coo_data + nnz);
+    r.resize(npad, c.coo_row_id[nnz - 1]);
+    cl.resize(npad, c.coo_col_id[nnz - 1]);
+    v.resize(npad, 0.0f);
+    p.npad = npad;
+    p.nwarps = (npad + dev::kCooChunk - 1) / dev::kCooChunk;
+    int rc;
+    if ((rc = upload_int(&p.i0, r.data(), npad, npad)) || (rc = upload_int(&p.i1, cl.data(), npad, npad)) ||
+        (rc = upload_val(&p.v, v.data(), npad, npad)))
+        return rc;
+    if ((rc = alloc(reinterpret_cast<void**>(&p.scratch_row), (size_t)2 * p.nwarps * sizeof(int))) ||
+        (rc = alloc(reinterpret_cast<void**>(&p.scratch_val), (size_t)2 * p.nwarps * sizeof(float))))
+        return rc;
+    parts.push_back(p);
+    return CSP_OK;
+}
+
+int Engine::add_ell(const ell_matrix_if& e, int method)
+{
+    const int m = e.matinfo.height;
+    if (e.ell_num < 0 || e.ell_height_aligned < m || (e.ell_num > 0 && (!e.ell_col_id || !e.ell_data)))
+        return set_error(CSP_EINVAL, "ELL part: bad fields");
+    Part p;
+    p.kind = PART_ELL;
+    p.method = (method == 1 && e.ell_height_aligned % 4 == 0) ? 1 : 0;
+    p.m = m;
+    p.k = e.ell_num;
+    p.stride = e.ell_height_aligned;
+    const size_t n = (size_t)e.ell_num * e.ell_height_aligned;
+    int rc;
+    if ((rc = upload_int(&p.i1, e.ell_col_id, n, n)) || (rc = upload_val(&p.v, e.ell_data, n, n))) return rc;
+    parts.push_back(p);
+    return CSP_OK;
+}
+
+int Engine::add_sell(const sell_matrix_if& s, int method)
+{
+    const int m = s.matinfo.height;
+    const int H = (int)s.sell_slice_height;
+    if (H <= 0 || s.sell_slice_num * (long long)H < m || !s.sell_slice_ptr) return set_error(CSP_EINVAL, "SELL part: bad fields");
+    const int total = s.sell_slice_ptr[s.sell_slice_num];
+    if (total > 0 && (!s.sell_col_id || !s.sell_data)) return set_error(CSP_EINVAL, "SELL part: bad arrays");
+    Part p;
+    p.kind = PART_SELL;
+    p.method = (method != 2 && H % 4 == 0) ? 1 : 0;  // 1: four rows per thread
+    p.m = m;
+    p.stride = H;
+    int rc;
+    if ((rc = upload_int(&p.i0, s.sell_slice_ptr, (size_t)s.sell_slice_num + 1, (size_t)s.sell_slice_num + 1)) ||
+        (rc = upload_int(&p.i1, s.sell_col_id, total, total)) || (rc = upload_val(&p.v, s.sell_data, total, total)))
+        return rc;
+    parts.push_back(p);
+    return CSP_OK;
+}
+
+int Engine::add_dia(const dia_matrix_iif& d, int method)
+{
+    const int len = d.dia_length_aligned;
+    if (d.dia_num < 0 || len < 0 || (d.dia_num > 0 && (!d.dia_offsets || !d.dia_data)))
+        return set_error(CSP_EINVAL, "DIA part: bad fields");
+    Part p;
+    p.kind = PART_DIA;
+    p.m = std::min(std::min(d.matinfo.height, height), len);
+    p.k = d.dia_num;
+    p.stride = len;
+    p.method = ((method == 1 || method == 3) && len % 4 == 0) ? 1 : 0;
+    const size_t n = (size_t)d.dia_num * len;
+    int rc;
+    if ((rc = upload_int(&p.i0, d.dia_offsets, d.dia_num, d.dia_num)) || (rc = upload_val(&p.v, d.dia_data, n, n))) return rc;
+    parts.push_back(p);
+    return CSP_OK;
+}
+
+int Engine::add_bdia(const bdia_matrix_iif& b, int method)
+{
+    const int len = b.bdia_length_aligned;
+    if (b.bdia_band_num < 0 || len < 0 || (b.bdia_band_num > 0 && (!b.bdia_offsets || !b.bdia_bptr || !b.bdia_data)))
+        return set_error(CSP_EINVAL, "BDIA part: bad fields");
+    Part p;
+    p.kind = PART_BDIA;
+    p.m = std::min(std::min(b.matinfo.height, height), len);
+    p.k = b.bdia_band_num;
+    p.stride = len;
+    const int ndia = b.bdia_band_num ? b.bdia_bptr[b.bdia_band_num] : 0;
+    int maxw = 1;
+    for (int i = 0; i < b.bdia_band_num; i++) maxw = std::max(maxw, b.bdia_bptr[i + 1] - b.bdia_bptr[i]);
+    p.maxw = maxw;
+    // reference numbering (spmv_cocktail.cpp:339-358): 0 nlvec, 1 staged, 2 staged (g4),
+    // 3 v4_nlvec, 4 v4 staged
+    p.method = ((method == 0 || method == 3) && len % 4 == 0) ? 0 : 1;
+    const size_t n = (size_t)ndia * len;
+    int rc;
+    if ((rc = upload_int(&p.i0, b.bdia_offsets, b.bdia_band_num, b.bdia_band_num)) ||
+        (rc = upload_int(&p.i1, b.bdia_bptr, (size_t)b.bdia_band_num + 1, (size_t)b.bdia_band_num + 1)) ||
+        (rc = upload_val(&p.v, b.bdia_data, n, n)))
+        return rc;
+    parts.push_back(p);
+    return CSP_OK;
+}
+
+static bool b4_shape_ok(unsigned bw, unsigned bh)
+{
+    return (bw == 4 || bw == 8) && (bh == 1 || bh == 2 || bh == 4 || bh == 8);
+}
+
+int Engine::add_bell(const b4ell_matrix_if& b, int method)
+{
+    if (!b4_shape_ok(b.b4ell_bwidth, b.b4ell_bheight)) return set_error(CSP_EUNSUP, "BELL part: block %ux%u", b.b4ell_bheight, b.b4ell_bwidth);
+    if (b.b4ell_float4_aligned % 4 != 0 || b.b4ell_float4_aligned < 4 * b.b4ell_row_num || b.b4ell_height_aligned < b.b4ell_row_num)
+        return set_error(CSP_EINVAL, "BELL part: bad alignment");
+    Part p;
+    p.kind = PART_BELL;
+    p.method = method;
+    p.bw = (int)b.b4ell_bwidth;
+    p.bh = (int)b.b4ell_bheight;
+    p.m = b.matinfo.height;
+    p.nbr = b.b4ell_row_num;
+    p.k = b.b4ell_block_num;
+    p.stride = b.b4ell_height_aligned;
+    p.f4 = b.b4ell_float4_aligned;
+    const size_t nc = (size_t)b.b4ell_height_aligned * b.b4ell_block_num;
+    const size_t nd = (size_t)b.b4ell_float4_aligned * b.b4ell_bheight * (b.b4ell_bwidth / 4) * b.b4ell_block_num;
+    int rc;
+    if ((rc = upload_int(&p.i1, b.b4ell_col_id, nc, nc)) || (rc = upload_val(&p.v, b.b4ell_data, nd, nd))) return rc;
+    parts.push_back(p);
+    return CSP_OK;
+}
+
+int Engine::add_sbell(const sbell_matrix_if& s, int method)
+{
+    if (!b4_shape_ok(s.sbell_bwidth, s.sbell_bheight)) return set_error(CSP_EUNSUP, "SBELL part: block %ux%u", s.sbell_bheight, s.sbell_bwidth);
+    if (s.sbell_slice_height == 0 || !s.sbell_slice_ptr || s.sbell_slice_num * (long long)s.sbell_slice_height < s.sbell_row_num)
+        return set_error(CSP_EINVAL, "SBELL part: bad fields");
+    Part p;
+    p.kind = PART_SBELL;
+    p.method = method;
+    p.bw = (int)s.sbell_bwidth;
+    p.bh = (int)s.sbell_bheight;
+    p.m = s.matinfo.height;
+    p.nbr = s.sbell_row_num;
+    p.stride = (int)s.sbell_slice_height;
+    const int total = s.sbell_slice_ptr[s.sbell_slice_num];
+    const size_t nd = (size_t)total * s.sbell_bwidth * s.sbell_bheight;
+    int rc;
+    if ((rc = upload_int(&p.i0, s.sbell_slice_ptr, (size_t)s.sbell_slice_num + 1, (size_t)s.sbell_slice_num + 1)) ||
+        (rc = upload_int(&p.i1, s.sbell_col_id, total, total)) || (rc = upload_val(&p.v, s.sbell_data, nd, nd)))
+        return rc;
+    parts.push_back(p);
+    return CSP_OK;
+}
+
+int Engine::add_bcsr(const b4csr_matrix_if& b, int method)
+{
+    if (!b4_shape_ok(b.b4csr_bwidth, b.b4csr_bheight)) return set_error(CSP_EUNSUP, "BCSR part: block %ux%u", b.b4csr_bheight, b.b4csr_bwidth);
+    if (b.b4csr_aligned_size % 4 != 0 || b.b4csr_aligned_size < 4 * b.b4csr_block_num || !b.b4csr_row_ptr)
+        return set_error(CSP_EINVAL, "BCSR part: bad alignment");
+    Part p;
+    p.kind = PART_BCSR;
+    p.method = method;
+    p.bw = (int)b.b4csr_bwidth;
+    p.bh = (int)b.b4csr_bheight;
+    p.m = b.matinfo.height;
+    p.nbr = b.b4csr_row_num;
+    p.stride = b.b4csr_aligned_size;
+    const size_t nd = (size_t)b.b4csr_aligned_size * b.b4csr_bheight * (b.b4csr_bwidth / 4);
+    int rc;
+    if ((rc = upload_int(&p.i0, b.b4csr_row_ptr, (size_t)b.b4csr_row_num + 1, (size_t)b.b4csr_row_num + 1)) ||
+        (rc = upload_int(&p.i1, b.b4csr_col_id, b.b4csr_block_num, b.b4csr_block_num)) ||
+        (rc = upload_val(&p.v, b.b4csr_data, nd, nd)))
+        return rc;
+    parts.push_back(p);
+    return CSP_OK;
+}
+
+int Engine::add_generic_bcsr(const bcsr_matrix_if& b, int method)
+{
+    const unsigned bw = b.bcsr_bwidth, bh = b.bcsr_bheight;
+    if (!((bh == 3 && bw == 3) || (bh == 2 && bw == 2) || (bh == 4 && bw == 4) || (bh == 1 && bw == 1) || (bh == 6 && bw == 6) ||
+          (bh == 8 && bw == 8)))
+        return set_error(CSP_EUNSUP, "generic BCSR: block %ux%u not compiled", bh, bw);
+    if (!b.bcsr_row_ptr || b.bcsr_aligned_size < b.bcsr_block_num) return set_error(CSP_EINVAL, "generic BCSR: bad fields");
+    Part p;
+    p.kind = PART_GBCSR;
+    p.method = method;
+    p.bw = (int)bw;
+    p.bh = (int)bh;
+    p.m = b.matinfo.height;
+    p.nbr = b.bcsr_row_num;
+    p.stride = b.bcsr_aligned_size;
+    const size_t nd = (size_t)b.bcsr_aligned_size * bw * bh;
+    int rc;
+    if ((rc = upload_int(&p.i0, b.bcsr_row_ptr, (size_t)b.bcsr_row_num + 1, (size_t)b.bcsr_row_num + 1)) ||
+        (rc = upload_int(&p.i1, b.bcsr_col_id, b.bcsr_block_num, b.bcsr_block_num)) ||
+        (rc = upload_val(&p.v, b.bcsr_data, nd, nd)))
+        return rc;
+    parts.push_back(p);
+    return CSP_OK;
+}
+
+// --------------------------------------------------------------------------
+// Launches
+// --------------------------------------------------------------------------
+template <class V>
+static void launch_part(const Part& p, const float* x, float* y, int n, cudaStream_t st)
+{
+    using namespace dev;
+    const V* v = static_cast<const V*>(p.v);
+    switch (p.kind) {
+    case PART_CSR: {
+        if (p.m == 0) return;
+        switch (p.method) {
+        case 0: csr_vector_kernel<V, 32><<<grid_for((long long)p.m * 32, 256), 256, 0, st>>>(p.i0, p.i1, v, x, y, p.m); break;
+        case 1: csr_block_row_kernel<V, 128><<<p.m, 128, 0, st>>>(p.i0, p.i1, v, x, y, p.m); break;
+        case 2: csr_adaptive_kernel<V><<<p.nblocks, kAdaptThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.i2); break;
+        case 3: {
+            const unsigned g = grid_for((long long)p.m * p.group, 256);
+            switch (p.group) {
+            case 2: csr_vector_kernel<V, 2><<<g, 256, 0, st>>>(p.i0, p.i1, v, x, y, p.m); break;
+            case 4: csr_vector_kernel<V, 4><<<g, 256, 0, st>>>(p.i0, p.i1, v, x, y, p.m); break;
+            case 8: csr_vector_kernel<V, 8><<<g, 256, 0, st>>>(p.i0, p.i1, v, x, y, p.m); break;
+            case 16: csr_vector_kernel<V, 16><<<g, 256, 0, st>>>(p.i0, p.i1, v, x, y, p.m); break;
+            default: csr_vector_kernel<V, 32><<<g, 256, 0, st>>>(p.i0, p.i1, v, x, y, p.m); break;
+            }
+            break;
+        }
+        case 4: csr_scalar_kernel<V, 1><<<grid_for(p.m, 256), 256, 0, st>>>(p.i0, p.i1, v, x, y, p.m); break;
+        case 5: csr_scalar_kernel<V, 4><<<grid_for(p.m, 256), 256, 0, st>>>(p.i0, p.i1, v, x, y, p.m); break;
+        case 6: csr_scalar4_kernel<V><<<grid_for(p.m, 256), 256, 0, st>>>(p.i0, p.i1, v, x, y, p.m); break;
+        }
+        break;
+    }
+    case PART_COO: {
+        coo_segment_kernel<V><<<grid_for((long long)p.nwarps * 32, 256), 256, 0, st>>>(p.i0, p.i1, v, x, y, p.npad, p.nwarps,
+                                                                                      p.scratch_row, p.scratch_val);
+        coo_fixup_kernel<<<grid_for(2LL * p.nwarps, 256), 256, 0, st>>>(p.scratch_row, p.scratch_val, 2 * p.nwarps, y);
+        break;
+    }
+    case PART_ELL:
+        if (p.m == 0) return;
+        if (p.method == 1) ell_kernel<V, 4><<<grid_for((p.m + 3) / 4, 256), 256, 0, st>>>(p.i1, v, x, y, p.m, p.k, p.stride);
+        else ell_kernel<V, 1><<<grid_for(p.m, 256), 256, 0, st>>>(p.i1, v, x, y, p.m, p.k, p.stride);
+        break;
+    case PART_SELL:
+        if (p.m == 0) return;
+        if (p.method == 1) sell4_kernel<V><<<grid_for((p.m + 3) / 4, 256), 256, 0, st>>>(p.i0, p.i1, v, x, y, p.m, p.stride);
+        else sell1_kernel<V><<<grid_for(p.m, 256), 256, 0, st>>>(p.i0, p.i1, v, x, y, p.m, p.stride);
+        break;
+    case PART_DIA: {
+        if (p.m == 0) return;
+        const size_t sm = (size_t)std::max(p.k, 1) * sizeof(int);
+        if (p.method == 1) dia4_kernel<V><<<grid_for((p.m + 3) / 4, kDiaThreads), kDiaThreads, sm, st>>>(p.i0, v, x, y, p.m, n, p.k, p.stride);
+        else dia_kernel<V, 2><<<grid_for(p.m, kDiaThreads * 2), kDiaThreads, sm, st>>>(p.i0, v, x, y, p.m, n, p.k, p.stride);
+        break;
+    }
+    case PART_BDIA: {
+        if (p.m == 0) return;
+        if (p.method == 0) {
+            bdia4_kernel<V><<<grid_for((p.m + 3) / 4, kDiaThreads), kDiaThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.m, n, p.k, p.stride);
+        } else {
+            const size_t sm = (size_t)(kDiaThreads * 4 + p.maxw) * sizeof(float);
+            bdia_staged_kernel<V, 4><<<grid_for(p.m, kDiaThreads * 4), kDiaThreads, sm, st>>>(p.i0, p.i1, v, x, y, p.m, n, p.k, p.stride);
+        }
+        break;
+    }
+    case PART_BELL: {
+        if (p.nbr == 0) return;
+        const unsigned g = grid_for(p.nbr, 256);
+#define CSP_BELL(BH, BW4) bell_b4_kernel<V, BH, BW4><<<g, 256, 0, st>>>(p.i1, v, x, y, p.nbr, p.k, p.stride, p.f4, p.m)
+        const int key = p.bh * 10 + p.bw / 4;
+        switch (key) {
+        case 11: CSP_BELL(1, 1); break; case 21: CSP_BELL(2, 1); break; case 41: CSP_BELL(4, 1); break; case 81: CSP_BELL(8, 1); break;
+        case 12: CSP_BELL(1, 2); break; case 22: CSP_BELL(2, 2); break; case 42: CSP_BELL(4, 2); break; case 82: CSP_BELL(8, 2); break;
+        }
+#undef CSP_BELL
+        break;
+    }
+    case PART_SBELL: {
+        if (p.nbr == 0) return;
+        const unsigned g = grid_for(p.nbr, 256);
+#define CSP_SBELL(BH, BW4) sbell_b4_kernel<V, BH, BW4><<<g, 256, 0, st>>>(p.i0, p.i1, v, x, y, p.nbr, p.stride, p.m)
+        const int key = p.bh * 10 + p.bw / 4;
+        switch (key) {
+        case 11: CSP_SBELL(1, 1); break; case 21: CSP_SBELL(2, 1); break; case 41: CSP_SBELL(4, 1); break; case 81: CSP_SBELL(8, 1); break;
+        case 12: CSP_SBELL(1, 2); break; case 22: CSP_SBELL(2, 2); break; case 42: CSP_SBELL(4, 2); break; case 82: CSP_SBELL(8, 2); break;
+        }
+#undef CSP_SBELL
+        break;
+    }
+    case PART_BCSR: {
+        if (p.nbr == 0) return;
+        const int G = (p.method == 1) ? 32 : 8;
+        const unsigned g = grid_for((long long)p.nbr * G, 256);
+#define CSP_BCSR(BH, BW4)                                                                                                   \
+    do {                                                                                                                    \
+        if (G == 32) bcsr_b4_kernel<V, BH, BW4, 32><<<g, 256, 0, st>>>(p.i0, p.i1, v, x, y, p.nbr, p.stride, p.m);       \
+        else bcsr_b4_kernel<V, BH, BW4, 8><<<g, 256, 0, st>>>(p.i0, p.i1, v, x, y, p.nbr, p.stride, p.m);                \
+    } while (0)
+        const int key = p.bh * 10 + p.bw / 4;
+        switch (key) {
+        case 11: CSP_BCSR(1, 1); break; case 21: CSP_BCSR(2, 1); break; case 41: CSP_BCSR(4, 1); break; case 81: CSP_BCSR(8, 1); break;
+        case 12: CSP_BCSR(1, 2); break; case 22: CSP_BCSR(2, 2); break; case 42: CSP_BCSR(4, 2); break; case 82: CSP_BCSR(8, 2); break;
+        }
+#undef CSP_BCSR
+        break;
+    }
+    case PART_GBCSR: {
+        if (p.nbr == 0) return;
+        const unsigned g = grid_for((long long)p.nbr * 8, 256);
+#define CSP_GB(BH, BW) bcsr_generic_kernel<V, BH, BW, 8><<<g, 256, 0, st>>>(p.i0, p.i1, v, x, y, p.nbr, p.stride, p.m, n)
+        switch (p.bh * 10 + p.bw) {
+        case 11: CSP_GB(1, 1); break; case 22: CSP_GB(2, 2); break; case 33: CSP_GB(3, 3); break;
+        case 44: CSP_GB(4, 4); break; case 66: CSP_GB(6, 6); break; case 88: CSP_GB(8, 8); break;
+        }
+#undef CSP_GB
+        break;
+    }
+    }
+}
+
+int Engine::launches_per_spmv() const
+{
+    int n = 0;
+    for (const Part& p : parts) n += (p.kind == PART_COO) ? 2 : 1;
+    return n;
+}
+
+int Engine::enqueue_once(cudaStream_t st)
+{
+    for (const Part& p : parts) {
+        if (bf16) launch_part<__nv_bfloat16>(p, d_x, d_y, width, st);
+        else launch_part<float>(p, d_x, d_y, width, st);
+    }
+    CSP_CUDA(cudaGetLastError());
+    return CSP_OK;
+}
+
+int Engine::spmv(int ntimes)
+{
+    if (ntimes < 0) return set_error(CSP_EINVAL, "ntimes < 0");
+    cudaStream_t st = stream;
+    if (!use_graph) {
+        for (int i = 0; i < ntimes; i++) {
+            int rc = enqueue_once(st);
+            if (rc) return rc;
+        }
+        return CSP_OK;
+    }
+    if (!graph_exec || graph_stream != st) {
+        if (graph_exec) { cudaGraphExecDestroy(graph_exec); graph_exec = nullptr; }
+        cudaGraph_t g;
+        CSP_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        int rc = enqueue_once(st);
+        cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (rc) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
+        if (e != cudaSuccess) return cuda_error(e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&graph_exec, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_error(e, "cudaGraphInstantiate");
+        graph_stream = st;
+    }
+    for (int i = 0; i < ntimes; i++) CSP_CUDA(cudaGraphLaunch(graph_exec, st));
+    return CSP_OK;
+}
+
+int Engine::init(const cocktail_iif* mat, const float* vec, const float* res, int flags)
+{
+    if (!mat) return set_error(CSP_EINVAL, "null cocktail");
+    width = mat->mat_width;
+    height = mat->mat_height;
+    nnz = mat->mat_nnz;
+    if (width < 0 || height < 0) return set_error(CSP_EINVAL, "negative matrix size");
+    bf16 = (flags & CSP_FLAG_BF16) != 0;
+    use_graph = (flags & CSP_FLAG_GRAPH) != 0;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return set_error(CSP_ENODEV, "no CUDA device: %s", cudaGetErrorString(e));
+    CSP_CUDA(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking));
+    stream = own_stream;
+    // x: zero-padded to a multiple of 64 (block kernels read float4s up to the padded width);
+    // y: padded to a multiple of 1024 like the reference (spmv_cocktail.cpp:234)
+    x_len = pad_to(std::max(width, 1), 64) + 64;
+    y_len = pad_to(std::max(height, 1), 1024);
+    int rc;
+    if ((rc = alloc(reinterpret_cast<void**>(&d_x), (size_t)x_len * 4)) || (rc = alloc(reinterpret_cast<void**>(&d_y), (size_t)y_len * 4)))
+        return rc;
+    CSP_CUDA(cudaMemset(d_x, 0, (size_t)x_len * 4));
+    CSP_CUDA(cudaMemset(d_y, 0, (size_t)y_len * 4));
+    if (vec && width) CSP_CUDA(cudaMemcpy(d_x, vec, (size_t)width * 4, cudaMemcpyHostToDevice));
+    if (res && height) CSP_CUDA(cudaMemcpy(d_y, res, (size_t)height * 4, cudaMemcpyHostToDevice));
+    // parts, in the reference's launch order
+    if (mat->ifusebdia && (rc = add_bdia(mat->bdia, mat->bdia_meth_num))) return rc;
+    if (mat->ifusedia && (rc = add_dia(mat->dia, mat->dia_meth_num))) return rc;
+    if (mat->ifusesbell && (rc = add_sbell(mat->sbell, mat->sbell_meth_num))) return rc;
+    if (mat->ifusebell && (rc = add_bell(mat->bell, mat->bell_meth_num))) return rc;
+    if (mat->ifusebcsr && (rc = add_bcsr(mat->bcsr, mat->bcsr_meth_num))) return rc;
+    if (mat->ifusesell && (rc = add_sell(mat->sell, mat->sell_meth_num))) return rc;
+    if (mat->ifuseell && (rc = add_ell(mat->ell, mat->ell_meth_num))) return rc;
+    if (mat->ifusecsr && (rc = add_csr(mat->csr, mat->csr_meth_num))) return rc;
+    if (mat->ifusecoo && (rc = add_coo(mat->coo))) return rc;
+    CSP_CUDA(cudaDeviceSynchronize());
+    return CSP_OK;
+}
+
+}  // namespace csp
+
+// ==========================================================================
+// C ABI
+// ==========================================================================
+using csp::Engine;
+using csp::set_error;
+using csp::cuda_error;
+
+struct csp_handle {
+    Engine eng;
+};
+
+#define CSP_HANDLE_CHECK(h) \
+    do { if (!(h)) return set_error(CSP_EINVAL, "null handle"); } while (0)
+
+extern "C" {
+
+const char* csp_error_string(int code)
+{
+    switch (code) {
+    case CSP_OK: return "CSP_OK";
+    case CSP_EINVAL: return "CSP_EINVAL";
+    case CSP_ENOMEM: return "CSP_ENOMEM";
+    case CSP_ECUDA: return "CSP_ECUDA";
+    case CSP_EFORMAT: return "CSP_EFORMAT";
+    case CSP_ENODEV: return "CSP_ENODEV";
+    case CSP_EUNSUP: return "CSP_EUNSUP";
+    case CSP_EIO: return "CSP_EIO";
+    case CSP_ETIMEOUT: return "CSP_ETIMEOUT";
+    default: return "CSP_E?";
+    }
+}
+
+const char* csp_last_error(void) { return csp::g_last_error.c_str(); }
+const char* csp_version(void) { return "clspmv_b200 0.1.0 (sm_100a)"; }
+
+int csp_init_mat_kernels(const cocktail_iif* mat, const float* vec, const float* res, int flags, csp_handle** out)
+{
+    if (!out) return set_error(CSP_EINVAL, "null output handle");
+    *out = nullptr;
+    csp_handle* h = new (std::nothrow) csp_handle();
+    if (!h) return set_error(CSP_ENOMEM, "handle");
+    int rc = h->eng.init(mat, vec, res, flags);
+    if (rc) { delete h; return rc; }
+    *out = h;
+    return CSP_OK;
+}
+
+int csp_do_spmv(csp_handle* h, int ntimes) { CSP_HANDLE_CHECK(h); return h->eng.spmv(ntimes); }
+
+int csp_synchronize(csp_handle* h)
+{
+    CSP_HANDLE_CHECK(h);
+    cudaError_t e = cudaStreamSynchronize(h->eng.stream);
+    return e == cudaSuccess ? CSP_OK : cuda_error(e, "cudaStreamSynchronize");
+}
+
+static int copy_in(csp_handle* h, float* dst, int cap, const void* src, int n, cudaMemcpyKind kind)
+{
+    if (!src || n < 0 || n > cap) return set_error(CSP_EINVAL, "copy of %d elements into a buffer of %d", n, cap);
+    cudaError_t e = cudaMemcpyAsync(dst, src, (size_t)n * 4, kind, h->eng.stream);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMemcpyAsync");
+    // a pageable host source may be reused by the caller on return
+    if (kind == cudaMemcpyHostToDevice) {
+        e = cudaStreamSynchronize(h->eng.stream);
+        if (e != cudaSuccess) return cuda_error(e, "cudaStreamSynchronize");
+    }
+    return CSP_OK;
+}
+
+int csp_cpy_vector_from_cpu(csp_handle* h, const float* vec, int n)
+{
+    CSP_HANDLE_CHECK(h);
+    return copy_in(h, h->eng.d_x, h->eng.width, vec, n, cudaMemcpyHostToDevice);
+}
+int csp_cpy_vector_from_gpu(csp_handle* h, const float* dvec, int n)
+{
+    CSP_HANDLE_CHECK(h);
+    return copy_in(h, h->eng.d_x, h->eng.width, dvec, n, cudaMemcpyDeviceToDevice);
+}
+int csp_cpy_result_from_cpu(csp_handle* h, const float* res, int n)
+{
+    CSP_HANDLE_CHECK(h);
+    return copy_in(h, h->eng.d_y, h->eng.height, res, n, cudaMemcpyHostToDevice);
+}
+int csp_cpy_result_from_gpu(csp_handle* h, const float* dres, int n)
+{
+    CSP_HANDLE_CHECK(h);
+    return copy_in(h, h->eng.d_y, h->eng.height, dres, n, cudaMemcpyDeviceToDevice);
+}
+int csp_cpy_result_to_cpu(csp_handle* h, float* res, int n)
+{
+    CSP_HANDLE_CHECK(h);
+    if (!res || n < 0 || n > h->eng.height) return set_error(CSP_EINVAL, "bad result copy");
+    cudaError_t e = cudaMemcpyAsync(res, h->eng.d_y, (size_t)n * 4, cudaMemcpyDeviceToHost, h->eng.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->eng.stream);
+    return e == cudaSuccess ? CSP_OK : cuda_error(e, "result to cpu");
+}
+int csp_cpy_result_to_gpu(csp_handle* h, float* dres, int n)
+{
+    CSP_HANDLE_CHECK(h);
+    if (!dres || n < 0 || n > h->eng.height) return set_error(CSP_EINVAL, "bad result copy");
+    cudaError_t e = cudaMemcpyAsync(dres, h->eng.d_y, (size_t)n * 4, cudaMemcpyDeviceToDevice, h->eng.stream);
+    return e == cudaSuccess ? CSP_OK : cuda_error(e, "result to gpu");
+}
+
+int csp_free_mat_kernels(csp_handle* h)
+{
+    if (!h) return CSP_OK;
+    cudaStreamSynchronize(h->eng.stream);
+    delete h;
+    return CSP_OK;
+}
+
+int csp_get_vec_device_ptr(csp_handle* h, float** p) { CSP_HANDLE_CHECK(h); if (!p) return set_error(CSP_EINVAL, "null"); *p = h->eng.d_x; return CSP_OK; }
+int csp_get_res_device_ptr(csp_handle* h, float** p) { CSP_HANDLE_CHECK(h); if (!p) return set_error(CSP_EINVAL, "null"); *p = h->eng.d_y; return CSP_OK; }
+
+int csp_set_stream(csp_handle* h, void* stream)
+{
+    CSP_HANDLE_CHECK(h);
+    h->eng.stream = stream ? static_cast<cudaStream_t>(stream) : h->eng.own_stream;
+    return CSP_OK;
+}
+int csp_get_stream(csp_handle* h, void** stream) { CSP_HANDLE_CHECK(h); if (!stream) return set_error(CSP_EINVAL, "null"); *stream = h->eng.stream; return CSP_OK; }
+int csp_launches_per_spmv(csp_handle* h, int* n) { CSP_HANDLE_CHECK(h); if (!n) return set_error(CSP_EINVAL, "null"); *n = h->eng.launches_per_spmv(); return CSP_OK; }
+int csp_device_bytes(csp_handle* h, size_t* b) { CSP_HANDLE_CHECK(h); if (!b) return set_error(CSP_EINVAL, "null"); *b = h->eng.device_bytes; return CSP_OK; }
+
+}  // extern "C"

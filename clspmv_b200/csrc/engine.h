@@ -1,0 +1,75 @@
+// Device engine state shared by the engine, driver and adjoint translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <vector>
+
+#include "csp/clspmv.h"
+
+namespace csp {
+
+enum PartKind { PART_BDIA, PART_DIA, PART_SBELL, PART_BELL, PART_BCSR, PART_SELL, PART_ELL, PART_CSR, PART_COO, PART_GBCSR };
+
+// One uploaded sub-matrix and its launch parameters.
+struct Part {
+    PartKind kind = PART_CSR;
+    int method = 0;
+    int* i0 = nullptr;   // row_ptr / slice_ptr / offsets / COO rows
+    int* i1 = nullptr;   // col ids / band pointers / COO cols
+    int* i2 = nullptr;   // CSR adaptive row blocks
+    void* v = nullptr;   // values (FP32 or BF16)
+    int* scratch_row = nullptr;   // COO chunk heads/tails
+    float* scratch_val = nullptr;
+    int m = 0;        // rows (or block rows' parent height)
+    int nnz = 0;
+    int k = 0;        // ELL width / #diagonals / #bands / BELL slots
+    int stride = 0;   // ELL/DIA aligned height, SELL/SBELL slice height, BELL height_aligned, BCSR aligned size
+    int f4 = 0;       // BELL float4_aligned
+    int bw = 0, bh = 0, nbr = 0;
+    int maxw = 0;     // BDIA widest band
+    int group = 0;    // CSR sub-warp lanes per row
+    int nblocks = 0;  // CSR adaptive row blocks
+    int npad = 0, nwarps = 0;  // COO
+};
+
+struct Engine {
+    int width = 0, height = 0, nnz = 0;
+    bool bf16 = false;
+    bool use_graph = false;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    float* d_x = nullptr;
+    float* d_y = nullptr;
+    int x_len = 0, y_len = 0;
+    std::vector<Part> parts;
+    std::vector<void*> allocations;
+    size_t device_bytes = 0;
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaStream_t graph_stream = nullptr;
+
+    ~Engine();
+    int init(const cocktail_iif* mat, const float* vec, const float* res, int flags);
+    int spmv(int ntimes);
+    int enqueue_once(cudaStream_t st);
+    int launches_per_spmv() const;
+
+    int alloc(void** p, size_t bytes);
+    int upload_int(int** d, const int* h, size_t n, size_t cap);
+    int upload_val(void** d, const float* h, size_t n, size_t cap);
+
+    int add_csr(const csr_matrix_if& c, int method);
+    int add_coo(const coo_matrix_if& c);
+    int add_ell(const ell_matrix_if& e, int method);
+    int add_sell(const sell_matrix_if& s, int method);
+    int add_dia(const dia_matrix_iif& d, int method);
+    int add_bdia(const bdia_matrix_iif& b, int method);
+    int add_bell(const b4ell_matrix_if& b, int method);
+    int add_sbell(const sbell_matrix_if& s, int method);
+    int add_bcsr(const b4csr_matrix_if& b, int method);
+    int add_generic_bcsr(const bcsr_matrix_if& b, int method);
+};
+
+int cuda_error(cudaError_t e, const char* what);
+
+}  // namespace csp

@@ -1,0 +1,378 @@
+/*
+ * clspmv_b200 -- C ABI of the B200 (sm_100a) Cocktail SpMV library.
+ *
+ * The library computes res += A * vec in FP32 (int32 indices) for a sparse
+ * matrix A stored in one or more of the nine clSpMV storage formats, exactly
+ * like clSpMV (clSpMV_NV/src/eval.cpp:40-42: the result buffer is accumulated,
+ * never overwritten).
+ *
+ * Struct layout.  Every matrix struct below has the same field names, field
+ * order and field types as the reference template instantiated at
+ * <int, float> (or <int, int, float>) in clSpMV_NV/include/matrix_storage.h,
+ * and `cocktail_iif` matches `cocktail<int, int, float>`
+ * (clSpMV_NV/include/analyze.h:105-144).  Code that fills the reference
+ * structs can pass them here unchanged.
+ *
+ * Conventions that differ from the reference:
+ *   - every function returns CSP_OK (0) or a CSP_E* code and never exits or
+ *     aborts (the reference calls exit(1) through CHECKERROR,
+ *     clSpMV_NV/include/oclcommon.h:11, or assert);
+ *   - OpenCL contexts/queues/cl_mem are replaced by an opaque csp_handle that
+ *     owns the device buffers and one CUDA stream;
+ *   - one handle per host thread; handles are not internally synchronised;
+ *   - csp_do_spmv is asynchronous on the handle's stream; the *_to_cpu copies
+ *     synchronise.
+ *
+ * Host arrays written by the conversion functions are malloc()ed by the
+ * library and released by the matching csp_free_* function, like the
+ * reference's init_/free_ pairs (matrix_storage.h:373-640).
+ */
+#ifndef CSP_CLSPMV_H
+#define CSP_CLSPMV_H
+
+#include <stddef.h>
+#include <stdbool.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+/* ------------------------------------------------------------------------ */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------ */
+#define CSP_OK        0
+#define CSP_EINVAL    1  /* invalid argument or inconsistent struct field        */
+#define CSP_ENOMEM    2  /* host or device allocation failed                     */
+#define CSP_ECUDA     3  /* a CUDA runtime call failed                           */
+#define CSP_EFORMAT   4  /* matrix not representable in the requested format    */
+#define CSP_ENODEV    5  /* no CUDA device is visible                            */
+#define CSP_EUNSUP    6  /* combination of options not supported                 */
+#define CSP_EIO       7  /* file could not be read or parsed                     */
+#define CSP_ETIMEOUT  8  /* a bounded device-side wait gave up                   */
+
+/* Human-readable name of a status code. */
+const char* csp_error_string(int code);
+/* Detail message of the last error raised on the calling thread ("" if none). */
+const char* csp_last_error(void);
+/* Library version string. */
+const char* csp_version(void);
+
+/* ------------------------------------------------------------------------ */
+/* Storage formats (layout-compatible with clSpMV_NV/include/matrix_storage.h) */
+/* ------------------------------------------------------------------------ */
+typedef struct matrixInfo_i { int width; int height; int nnz; } matrixInfo_i;  /* :15-25 */
+
+typedef struct dia_matrix_iif {                          /* matrix_storage.h:27-47 */
+    matrixInfo_i matinfo;
+    int dia_num;
+    int dia_length;
+    int dia_length_aligned;
+    int* dia_offsets;
+    float* dia_data;
+} dia_matrix_iif;
+
+typedef struct bdia_matrix_iif {                         /* matrix_storage.h:71-94 */
+    matrixInfo_i matinfo;
+    int bdia_band_num;
+    int bdia_length;
+    int bdia_length_aligned;
+    int* bdia_offsets;
+    int* bdia_bptr;
+    float* bdia_data;
+} bdia_matrix_iif;
+
+typedef struct ell_matrix_if {                           /* matrix_storage.h:96-111 */
+    matrixInfo_i matinfo;
+    int ell_num;
+    int ell_height_aligned;
+    int* ell_col_id;
+    float* ell_data;
+} ell_matrix_if;
+
+typedef struct sell_matrix_if {                          /* matrix_storage.h:114-137 */
+    matrixInfo_i matinfo;
+    unsigned int sell_slice_height;
+    int sell_slice_num;
+    int* sell_slice_ptr;
+    int* sell_col_id;
+    float* sell_data;
+} sell_matrix_if;
+
+typedef struct coo_matrix_if {                           /* matrix_storage.h:141-152 */
+    matrixInfo_i matinfo;
+    int* coo_row_id;
+    int* coo_col_id;
+    float* coo_data;
+} coo_matrix_if;
+
+typedef struct csr_matrix_if {                           /* matrix_storage.h:155-166 */
+    matrixInfo_i matinfo;
+    int* csr_row_ptr;
+    int* csr_col_id;
+    float* csr_data;
+} csr_matrix_if;
+
+typedef struct bcsr_matrix_if {                          /* matrix_storage.h:169-199 */
+    matrixInfo_i matinfo;
+    unsigned int bcsr_bwidth;
+    unsigned int bcsr_bheight;
+    int bcsr_row_num;
+    int bcsr_aligned_size;
+    int bcsr_block_num;
+    int* bcsr_row_ptr;
+    int* bcsr_col_id;
+    float* bcsr_data;
+} bcsr_matrix_if;
+
+typedef struct bell_matrix_if {                          /* matrix_storage.h:215-236 */
+    matrixInfo_i matinfo;
+    unsigned int bell_bwidth;
+    unsigned int bell_bheight;
+    int bell_row_num;
+    int bell_block_num;
+    int bell_height_aligned;
+    int bell_float4_aligned;
+    int* bell_col_id;
+    float* bell_data;
+} bell_matrix_if;
+
+typedef struct b4csr_matrix_if {                         /* matrix_storage.h:266-287 */
+    matrixInfo_i matinfo;
+    unsigned int b4csr_bwidth;
+    unsigned int b4csr_bheight;
+    int b4csr_row_num;
+    int b4csr_aligned_size;
+    int b4csr_block_num;
+    int* b4csr_row_ptr;
+    int* b4csr_col_id;
+    float* b4csr_data;
+} b4csr_matrix_if;
+
+typedef struct b4ell_matrix_if {                         /* matrix_storage.h:311-332 */
+    matrixInfo_i matinfo;
+    unsigned int b4ell_bwidth;
+    unsigned int b4ell_bheight;
+    int b4ell_row_num;
+    int b4ell_block_num;
+    int b4ell_height_aligned;
+    int b4ell_float4_aligned;
+    int* b4ell_col_id;
+    float* b4ell_data;
+} b4ell_matrix_if;
+
+typedef struct sbell_matrix_if {                         /* matrix_storage.h:344-365 */
+    matrixInfo_i matinfo;
+    unsigned int sbell_bwidth;
+    unsigned int sbell_bheight;
+    unsigned int sbell_slice_height;
+    int sbell_slice_num;
+    int sbell_row_num;
+    int* sbell_slice_ptr;
+    int* sbell_col_id;
+    float* sbell_data;
+} sbell_matrix_if;
+
+/* The Cocktail container: one optional sub-matrix per format plus the kernel
+ * variant ("method") chosen for each.  Layout of cocktail<int,int,float>,
+ * clSpMV_NV/include/analyze.h:105-144. */
+typedef struct cocktail_iif {
+    bool ifusebdia;
+    bool ifusedia;
+    bool ifusesbell;
+    bool ifusebell;
+    bool ifusebcsr;
+    bool ifusesell;
+    bool ifuseell;
+    bool ifusecsr;
+    bool ifusecoo;
+
+    int bdia_meth_num;
+    int dia_meth_num;
+    int sbell_meth_num;
+    int bell_meth_num;
+    int bcsr_meth_num;
+    int sell_meth_num;
+    int ell_meth_num;
+    int csr_meth_num;
+    int coo_meth_num;
+
+    int csr_group_num;
+    int coo_group_num;
+
+    int mat_width;
+    int mat_height;
+    int mat_nnz;
+
+    bdia_matrix_iif bdia;
+    dia_matrix_iif dia;
+    sbell_matrix_if sbell;
+    b4ell_matrix_if bell;
+    b4csr_matrix_if bcsr;
+    sell_matrix_if sell;
+    ell_matrix_if ell;
+    csr_matrix_if csr;
+    coo_matrix_if coo;
+} cocktail_iif;
+
+/* ------------------------------------------------------------------------ */
+/* init_ / free_ (matrix_storage.h:373-640; analyze.h:146-206)               */
+/* free_* releases the arrays only; the info fields stay, as in the reference. */
+/* ------------------------------------------------------------------------ */
+void csp_init_coo_matrix(coo_matrix_if* m);
+void csp_init_csr_matrix(csr_matrix_if* m);
+void csp_init_ell_matrix(ell_matrix_if* m);
+void csp_init_sell_matrix(sell_matrix_if* m);
+void csp_init_dia_matrix(dia_matrix_iif* m);
+void csp_init_bdia_matrix(bdia_matrix_iif* m);
+void csp_init_bcsr_matrix(bcsr_matrix_if* m);
+void csp_init_bell_matrix(bell_matrix_if* m);
+void csp_init_b4csr_matrix(b4csr_matrix_if* m);
+void csp_init_b4ell_matrix(b4ell_matrix_if* m);
+void csp_init_sbell_matrix(sbell_matrix_if* m);
+void csp_init_cocktail(cocktail_iif* m);
+
+void csp_free_coo_matrix(coo_matrix_if* m);
+void csp_free_csr_matrix(csr_matrix_if* m);
+void csp_free_ell_matrix(ell_matrix_if* m);
+void csp_free_sell_matrix(sell_matrix_if* m);
+void csp_free_dia_matrix(dia_matrix_iif* m);
+void csp_free_bdia_matrix(bdia_matrix_iif* m);
+void csp_free_bcsr_matrix(bcsr_matrix_if* m);
+void csp_free_bell_matrix(bell_matrix_if* m);
+void csp_free_b4csr_matrix(b4csr_matrix_if* m);
+void csp_free_b4ell_matrix(b4ell_matrix_if* m);
+void csp_free_sbell_matrix(sbell_matrix_if* m);
+void csp_free_cocktail(cocktail_iif* m);
+
+/* ------------------------------------------------------------------------ */
+/* Host-side conversions.  Output arrays are byte-identical to the reference */
+/* functions named beside each declaration, including padding values.        */
+/* Functions that the reference lets sort the input in place do the same.    */
+/* ------------------------------------------------------------------------ */
+int csp_aligned_length(int length, int alignment);                  /* matrix_storage.h:818 */
+int csp_if_sorted_coo(const coo_matrix_if* m);                       /* matrix_storage.h:732 */
+int csp_sort_coo(coo_matrix_if* m);                                  /* matrix_storage.h:745; CSP_EFORMAT on stack overflow */
+int csp_coo2csr(coo_matrix_if* src, csr_matrix_if* dst);             /* matrix_storage.h:1269 */
+int csp_csr2coo(const csr_matrix_if* src, coo_matrix_if* dst);       /* matrix_storage.h:1239 */
+int csp_coo2ell(coo_matrix_if* src, ell_matrix_if* dst, int alignment, int ellnum);   /* :1341 */
+int csp_ell2coo(const ell_matrix_if* src, coo_matrix_if* dst);       /* matrix_storage.h:1310 */
+int csp_coo2sell(coo_matrix_if* src, sell_matrix_if* dst, unsigned int sliceheight); /* :1398 */
+int csp_coo2dia(coo_matrix_if* src, dia_matrix_iif* dst, int alignment);             /* :937; CSP_EFORMAT when too padded */
+int csp_dia2coo(const dia_matrix_iif* src, coo_matrix_if* dst);      /* matrix_storage.h:826 */
+int csp_coo2bdia(coo_matrix_if* src, bdia_matrix_iif* dst, int alignment);           /* :1185 */
+int csp_bdia2coo(const bdia_matrix_iif* src, coo_matrix_if* dst);    /* matrix_storage.h:1137 */
+int csp_coo2bcsr(coo_matrix_if* src, bcsr_matrix_if* dst, unsigned int bwidth, unsigned int bheight, int alignment); /* :1595 */
+int csp_bcsr2coo(const bcsr_matrix_if* src, coo_matrix_if* dst);     /* matrix_storage.h:1546 */
+int csp_coo2bell(coo_matrix_if* src, bell_matrix_if* dst, unsigned int bwidth, unsigned int bheight, int alignment, int ellnum); /* :1941 */
+int csp_bell2coo(const bell_matrix_if* src, coo_matrix_if* dst);     /* matrix_storage.h:1901 */
+int csp_coo2b4csr(coo_matrix_if* src, b4csr_matrix_if* dst, unsigned int bwidth, unsigned int bheight, int alignment); /* :1741; CSP_EFORMAT above MAX_MEM_OBJ */
+int csp_coo2b4ell(coo_matrix_if* src, b4ell_matrix_if* dst, unsigned int bwidth, unsigned int bheight, int alignment, int ellnum); /* :2010 */
+int csp_coo2sbell(coo_matrix_if* src, sbell_matrix_if* dst, unsigned int bwidth, unsigned int bheight, unsigned int sliceheight); /* :2203 */
+int csp_pad_csr(const csr_matrix_if* src, csr_matrix_if* dst, int alignment);        /* util.cpp:31 */
+
+/* ------------------------------------------------------------------------ */
+/* Cocktail analyzer (analyze.h:257 analyze_matrix)                          */
+/* ------------------------------------------------------------------------ */
+#define CSP_ANALYZE_REFERENCE 0  /* reference decisions from clSpMV .ben tables      */
+#define CSP_ANALYZE_AUTOTUNE  1  /* B200 decisions: measured on the device, cached   */
+
+typedef struct csp_analyze_opts {
+    int mode;                /* CSP_ANALYZE_REFERENCE or CSP_ANALYZE_AUTOTUNE            */
+    const char* bench_path;  /* directory holding benchmark/ *.ben; NULL = $CLSPMVPATH     */
+    int verbose;             /* 0 = silent, 1 = print the reference's progress lines     */
+    const char* cache_path;  /* AUTOTUNE: file caching decisions per sparsity signature  */
+} csp_analyze_opts;
+
+/* Partition `coo` into the per-format sub-matrices of `mat`.  `coo` may be
+ * sorted in place (as the reference does).  opts may be NULL (REFERENCE mode,
+ * $CLSPMVPATH, silent). */
+int csp_analyze_matrix(coo_matrix_if* coo, cocktail_iif* mat, const csp_analyze_opts* opts);
+
+/* ------------------------------------------------------------------------ */
+/* Device engine (spmv_cocktail.h:111-175)                                   */
+/* ------------------------------------------------------------------------ */
+typedef struct csp_handle csp_handle;
+
+#define CSP_FLAG_USE_TEX   0x1  /* accepted for API compatibility; x is always read through the read-only path */
+#define CSP_FLAG_BF16      0x2  /* store matrix values as BF16, accumulate in FP32                             */
+#define CSP_FLAG_GRAPH     0x4  /* replay do_spmv as one captured CUDA graph                                   */
+#define CSP_FLAG_ADJOINT   0x8  /* also build the transposed structures for csp_spmv_adjoint                  */
+
+/* Upload every used sub-matrix of `mat`, x = vec (length mat_width) and
+ * res (length mat_height; may be NULL for zeros), and select one kernel per
+ * sub-matrix from its *_meth_num.  (spmv_cocktail.cpp:1593 init_mat_kernels) */
+int csp_init_mat_kernels(const cocktail_iif* mat, const float* vec, const float* res, int flags, csp_handle** out);
+/* Enqueue ntimes SpMVs res += A*vec on the handle's stream.  (:1091 do_spmv) */
+int csp_do_spmv(csp_handle* h, int ntimes);
+/* Block until every launch on the handle's stream has finished. */
+int csp_synchronize(csp_handle* h);
+int csp_cpy_vector_from_cpu(csp_handle* h, const float* vec, int vec_size);     /* :1462 */
+int csp_cpy_vector_from_gpu(csp_handle* h, const float* dvec, int vec_size);    /* :1513, dvec = device pointer */
+int csp_cpy_result_from_cpu(csp_handle* h, const float* res, int res_size);     /* :1562 */
+int csp_cpy_result_from_gpu(csp_handle* h, const float* dres, int res_size);    /* :1571 */
+int csp_cpy_result_to_cpu(csp_handle* h, float* res, int res_size);             /* :1578, synchronises */
+int csp_cpy_result_to_gpu(csp_handle* h, float* dres, int res_size);            /* :1585 */
+int csp_free_mat_kernels(csp_handle* h);                                        /* :1616 */
+
+/* Device pointers of the handle's x and res buffers (like gpumat.vec / gpumat.res). */
+int csp_get_vec_device_ptr(csp_handle* h, float** dvec);
+int csp_get_res_device_ptr(csp_handle* h, float** dres);
+/* Launch on a caller-owned cudaStream_t (passed as void*); NULL = the handle's own stream. */
+int csp_set_stream(csp_handle* h, void* stream);
+int csp_get_stream(csp_handle* h, void** stream);
+/* Number of kernel launches one csp_do_spmv(h, 1) enqueues. */
+int csp_launches_per_spmv(csp_handle* h, int* launches);
+/* Bytes of device memory the handle owns. */
+int csp_device_bytes(csp_handle* h, size_t* bytes);
+
+/* Correctness and timing of one engine against the serial COO result
+ * (spmv_cocktail.cpp:1434 evaluate / :1137 check_and_time).  Prints nothing;
+ * fills the report. */
+typedef struct csp_report {
+    int    method;          /* best kernel variant (format-specific numbering)    */
+    double gflops;          /* 2*nnz / best time                                  */
+    double gbytes;          /* algorithmic bytes / best time, GB/s                */
+    double ms;              /* best time per SpMV, milliseconds                   */
+    double l2_distance;     /* || y_gpu - y_coo ||_2   (util.cpp:93 two_vec_compare) */
+    double max_diff;        /* max | |y_gpu| - |y_coo| |                          */
+    double max_ratio_diff;  /* max of the relative form of the same               */
+    int    group_num;       /* CSR/COO: work-group count used                    */
+} csp_report;
+int csp_evaluate(const cocktail_iif* mat, const float* vec, const float* res, const float* coores, int ntimes, csp_report* report);
+
+/* ------------------------------------------------------------------------ */
+/* spmv_all single-format drivers (NV/include/spmv_*.h:7; spmv_all.cpp:196)   */
+/* method: 1 csr_scalar, 2 csr_vector, 3 bdia, 4 dia, 5 ell, 6 coo, 7 bell,   */
+/* 8 bcsr, 9 sell, 10 sbell (spmv_all.cpp:164-175).  Each converts `coo`, runs */
+/* every kernel variant                                                        */
+/* of that format (one checked launch, 3 warm-ups, ntimes timed) and reports   */
+/* the best, without printing.                                                 */
+/* ------------------------------------------------------------------------ */
+int csp_spmv_all(coo_matrix_if* coo, int method, int ntimes, csp_report* report);
+int csp_spmv_csr_scalar(coo_matrix_if* coo, int ntimes, csp_report* report);
+int csp_spmv_csr_vector(coo_matrix_if* coo, int ntimes, csp_report* report);
+int csp_spmv_bdia(coo_matrix_if* coo, int ntimes, csp_report* report);
+int csp_spmv_dia(coo_matrix_if* coo, int ntimes, csp_report* report);
+int csp_spmv_ell(coo_matrix_if* coo, int ntimes, csp_report* report);
+int csp_spmv_sell(coo_matrix_if* coo, int ntimes, csp_report* report);
+int csp_spmv_coo(coo_matrix_if* coo, int ntimes, csp_report* report);
+int csp_spmv_bell(coo_matrix_if* coo, int ntimes, csp_report* report);
+int csp_spmv_bcsr(coo_matrix_if* coo, int ntimes, csp_report* report);
+int csp_spmv_sbell(coo_matrix_if* coo, int ntimes, csp_report* report);
+
+/* ------------------------------------------------------------------------ */
+/* MatrixMarket input (fileio.cpp:10 ReadMMF): 0-based, pattern -> 1.0,       */
+/* symmetric mirrored, sorted.                                               */
+/* ------------------------------------------------------------------------ */
+int csp_read_mmf(const char* filename, coo_matrix_if* mat);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif /* CSP_CLSPMV_H */

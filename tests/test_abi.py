@@ -1,0 +1,57 @@
+"""The C ABI library loads without a GPU and exports every function the public
+headers declare; calls that need a device fail with CSP_ENODEV, not a crash."""
+import ctypes as C
+import glob
+import os
+import re
+
+import numpy as np
+
+from clspmv_b200 import COO, Cocktail, capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "csp", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"\b(csp_[a-z0-9_]+)\s*\(", text))
+    return sorted(names)
+
+
+def test_every_declared_symbol_is_exported(L):
+    names = declared_functions()
+    assert len(names) > 60
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_struct_sizes_match_reference_layout():
+    # cocktail<int,int,float>: 9 bools, 11+3 ints, then 9 sub-structs (LP64)
+    assert C.sizeof(capi.coo_matrix) == 40
+    assert C.sizeof(capi.csr_matrix) == 40
+    assert C.sizeof(capi.dia_matrix) == 40
+    assert C.sizeof(capi.bdia_matrix) == 48
+    assert C.sizeof(capi.b4ell_matrix) == 56
+    assert C.sizeof(capi.sbell_matrix) == 56
+
+
+def test_version_and_errors(L):
+    assert b"sm_100a" in L.csp_version()
+    assert L.csp_error_string(capi.CSP_EFORMAT) == b"CSP_EFORMAT"
+    assert L.csp_aligned_length(33, 32) == 64
+
+
+def test_device_calls_fail_cleanly_without_gpu(L):
+    import torch
+    if torch.cuda.is_available():
+        return
+    coo = COO(3, 3, [0, 1, 2], [0, 1, 2], [1, 2, 3])
+    mat = Cocktail.single("csr", coo)
+    h = C.c_void_p()
+    x = np.ones(3, np.float32)
+    rc = L.csp_init_mat_kernels(mat.ref(), capi.as_ptr(x, C.c_float), None, 0, C.byref(h))
+    assert rc in (capi.CSP_ENODEV, capi.CSP_ECUDA)
+    assert not h.value
