@@ -217,7 +217,9 @@ def main():
     h, w, r, c, v = case
     nnz = int(r.size)
     ab = algorithmic_bytes(h, w, nnz)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library and torch (flush, events) must launch on the same one
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
 
     def time_handle(hd: Handle, steps: int, warmup: int):

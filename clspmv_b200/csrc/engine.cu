@@ -118,6 +118,23 @@ Engine::~Engine()
 }
 
 static inline int pad_to(int v, int a) { return (v + a - 1) / a * a; }
+
+// Every column id a kernel will dereference must lie in [0, hi): a struct filled by
+// hand with a stray index is refused here instead of faulting on the device.
+static int check_ids(const int* ids, size_t n, long long hi, const char* what)
+{
+    for (size_t i = 0; i < n; i++)
+        if (ids[i] < 0 || ids[i] >= hi) return set_error(CSP_EINVAL, "%s: index %d at %zu outside [0, %lld)", what, ids[i], i, hi);
+    return CSP_OK;
+}
+
+static int check_row_ptr(const int* rp, int rows, const char* what)
+{
+    if (rp[0] != 0) return set_error(CSP_EINVAL, "%s: row pointer does not start at 0", what);
+    for (int i = 0; i < rows; i++)
+        if (rp[i + 1] < rp[i]) return set_error(CSP_EINVAL, "%s: row pointer decreases at %d", what, i);
+    return CSP_OK;
+}
 static inline unsigned grid_for(long long threads, int block) { return (unsigned)((threads + block - 1) / block); }
 
 // --------------------------------------------------------------------------
@@ -130,12 +147,14 @@ int Engine::add_csr(const csr_matrix_if& c, int method)
     const int nnz = c.csr_row_ptr[m];
     if (nnz < 0 || (nnz > 0 && (!c.csr_col_id || !c.csr_data))) return set_error(CSP_EINVAL, "CSR part: bad arrays");
     if (m > height) return set_error(CSP_EINVAL, "CSR part taller than the cocktail");
+    int rc;
+    if ((rc = check_row_ptr(c.csr_row_ptr, m, "CSR part")) || (rc = check_ids(c.csr_col_id, nnz, width, "CSR part")))
+        return rc;
     Part p;
     p.kind = PART_CSR;
     p.method = method;
     p.m = m;
     p.nnz = nnz;
-    int rc;
     if (method == 6) {
         // float4 scalar kernel on the row-padded CSR (util.cpp:31 pad_csr with 4)
         csr_matrix_if padded;
@@ -234,6 +253,8 @@ int Engine::add_ell(const ell_matrix_if& e, int method)
     p.stride = e.ell_height_aligned;
     const size_t n = (size_t)e.ell_num * e.ell_height_aligned;
     int rc;
+    if (m > height) return set_error(CSP_EINVAL, "ELL part taller than the cocktail");
+    if ((rc = check_ids(e.ell_col_id, n, width, "ELL part"))) return rc;   // the 4-row kernel reads alignment rows too
     if ((rc = upload_int(&p.i1, e.ell_col_id, n, n)) || (rc = upload_val(&p.v, e.ell_data, n, n))) return rc;
     parts.push_back(p);
     return CSP_OK;
@@ -252,6 +273,12 @@ int Engine::add_sell(const sell_matrix_if& s, int method)
     p.m = m;
     p.stride = H;
     int rc;
+    if (m > height) return set_error(CSP_EINVAL, "SELL part taller than the cocktail");
+    for (int i = 0; i < s.sell_slice_num; i++)
+        if (s.sell_slice_ptr[i + 1] < s.sell_slice_ptr[i] || (s.sell_slice_ptr[i + 1] - s.sell_slice_ptr[i]) % H != 0 ||
+            s.sell_slice_ptr[0] != 0)
+            return set_error(CSP_EINVAL, "SELL part: slice pointer %d inconsistent with slice height %d", i, H);
+    if ((rc = check_ids(s.sell_col_id, (size_t)total, width, "SELL part"))) return rc;
     if ((rc = upload_int(&p.i0, s.sell_slice_ptr, (size_t)s.sell_slice_num + 1, (size_t)s.sell_slice_num + 1)) ||
         (rc = upload_int(&p.i1, s.sell_col_id, total, total)) || (rc = upload_val(&p.v, s.sell_data, total, total)))
         return rc;
@@ -264,6 +291,7 @@ int Engine::add_dia(const dia_matrix_iif& d, int method)
     const int len = d.dia_length_aligned;
     if (d.dia_num < 0 || len < 0 || (d.dia_num > 0 && (!d.dia_offsets || !d.dia_data)))
         return set_error(CSP_EINVAL, "DIA part: bad fields");
+    if (d.dia_num > 12000) return set_error(CSP_EUNSUP, "DIA part: %d diagonals (at most 12000)", d.dia_num);
     Part p;
     p.kind = PART_DIA;
     p.m = std::min(std::min(d.matinfo.height, height), len);
@@ -294,6 +322,10 @@ int Engine::add_bdia(const bdia_matrix_iif& b, int method)
     // reference numbering (spmv_cocktail.cpp:339-358): 0 nlvec, 1 staged, 2 staged (g4),
     // 3 v4_nlvec, 4 v4 staged
     p.method = ((method == 0 || method == 3) && len % 4 == 0) ? 0 : 1;
+    if (maxw > 8000) p.method = 0;   // staged window would not fit in shared memory
+    if (p.method == 0 && len % 4 != 0) return set_error(CSP_EUNSUP, "BDIA part: band wider than 8000 with unaligned length");
+    for (int i = 0; i < b.bdia_band_num; i++)
+        if (b.bdia_bptr[i + 1] < b.bdia_bptr[i] || b.bdia_bptr[0] != 0) return set_error(CSP_EINVAL, "BDIA part: bad band pointer");
     const size_t n = (size_t)ndia * len;
     int rc;
     if ((rc = upload_int(&p.i0, b.bdia_offsets, b.bdia_band_num, b.bdia_band_num)) ||
@@ -327,6 +359,10 @@ int Engine::add_bell(const b4ell_matrix_if& b, int method)
     const size_t nc = (size_t)b.b4ell_height_aligned * b.b4ell_block_num;
     const size_t nd = (size_t)b.b4ell_float4_aligned * b.b4ell_bheight * (b.b4ell_bwidth / 4) * b.b4ell_block_num;
     int rc;
+    for (int k = 0; k < b.b4ell_block_num; k++)
+        if ((rc = check_ids(b.b4ell_col_id + (size_t)k * b.b4ell_height_aligned, (size_t)b.b4ell_row_num,
+                            (x_len - (long long)b.b4ell_bwidth) / 4 + 1, "BELL part")))
+            return rc;
     if ((rc = upload_int(&p.i1, b.b4ell_col_id, nc, nc)) || (rc = upload_val(&p.v, b.b4ell_data, nd, nd))) return rc;
     parts.push_back(p);
     return CSP_OK;
@@ -348,6 +384,11 @@ int Engine::add_sbell(const sbell_matrix_if& s, int method)
     const int total = s.sbell_slice_ptr[s.sbell_slice_num];
     const size_t nd = (size_t)total * s.sbell_bwidth * s.sbell_bheight;
     int rc;
+    for (int i = 0; i < s.sbell_slice_num; i++)
+        if (s.sbell_slice_ptr[0] != 0 || s.sbell_slice_ptr[i + 1] < s.sbell_slice_ptr[i] ||
+            (s.sbell_slice_ptr[i + 1] - s.sbell_slice_ptr[i]) % (int)s.sbell_slice_height != 0)
+            return set_error(CSP_EINVAL, "SBELL part: bad slice pointer");
+    if ((rc = check_ids(s.sbell_col_id, (size_t)total, (x_len - (long long)s.sbell_bwidth) / 4 + 1, "SBELL part"))) return rc;
     if ((rc = upload_int(&p.i0, s.sbell_slice_ptr, (size_t)s.sbell_slice_num + 1, (size_t)s.sbell_slice_num + 1)) ||
         (rc = upload_int(&p.i1, s.sbell_col_id, total, total)) || (rc = upload_val(&p.v, s.sbell_data, nd, nd)))
         return rc;
@@ -370,6 +411,9 @@ int Engine::add_bcsr(const b4csr_matrix_if& b, int method)
     p.stride = b.b4csr_aligned_size;
     const size_t nd = (size_t)b.b4csr_aligned_size * b.b4csr_bheight * (b.b4csr_bwidth / 4);
     int rc;
+    if ((rc = check_row_ptr(b.b4csr_row_ptr, b.b4csr_row_num, "BCSR part"))) return rc;
+    if (b.b4csr_row_ptr[b.b4csr_row_num] > b.b4csr_block_num) return set_error(CSP_EINVAL, "BCSR part: row pointer past the blocks");
+    if ((rc = check_ids(b.b4csr_col_id, (size_t)b.b4csr_block_num, (x_len - (long long)b.b4csr_bwidth) / 4 + 1, "BCSR part"))) return rc;
     if ((rc = upload_int(&p.i0, b.b4csr_row_ptr, (size_t)b.b4csr_row_num + 1, (size_t)b.b4csr_row_num + 1)) ||
         (rc = upload_int(&p.i1, b.b4csr_col_id, b.b4csr_block_num, b.b4csr_block_num)) ||
         (rc = upload_val(&p.v, b.b4csr_data, nd, nd)))
@@ -395,6 +439,9 @@ int Engine::add_generic_bcsr(const bcsr_matrix_if& b, int method)
     p.stride = b.bcsr_aligned_size;
     const size_t nd = (size_t)b.bcsr_aligned_size * bw * bh;
     int rc;
+    if ((rc = check_row_ptr(b.bcsr_row_ptr, b.bcsr_row_num, "generic BCSR"))) return rc;
+    if (b.bcsr_row_ptr[b.bcsr_row_num] > b.bcsr_block_num) return set_error(CSP_EINVAL, "generic BCSR: row pointer past the blocks");
+    if ((rc = check_ids(b.bcsr_col_id, (size_t)b.bcsr_block_num, width, "generic BCSR"))) return rc;
     if ((rc = upload_int(&p.i0, b.bcsr_row_ptr, (size_t)b.bcsr_row_num + 1, (size_t)b.bcsr_row_num + 1)) ||
         (rc = upload_int(&p.i1, b.bcsr_col_id, b.bcsr_block_num, b.bcsr_block_num)) ||
         (rc = upload_val(&p.v, b.bcsr_data, nd, nd)))

@@ -228,6 +228,21 @@ __global__ void __launch_bounds__(256) coo_segment_kernel(const int* __restrict_
         const float4 a = Val<V>::ld4(val + j);
         const float p0 = a.x * ldx(x, c.x), p1 = a.y * ldx(x, c.y);
         const float p2 = a.z * ldx(x, c.z), p3 = a.w * ldx(x, c.w);
+        // the segment carried out of the previous tile ends if this tile starts a new row
+        const int tile_first = __shfl_sync(0xffffffffu, r.x, 0);
+        if (tile_first != carry_row) {
+            if (lane == 0) {
+                if (head_open && carry_row == head_row) {
+                    part_row[2 * w] = carry_row;
+                    part_val[2 * w] = carry_val;
+                } else {
+                    y[carry_row] += carry_val;
+                }
+            }
+            if (head_open && carry_row == head_row) head_open = false;
+            carry_row = tile_first;
+            carry_val = 0.0f;
+        }
         // suffix run of this lane (entries equal to its last row)
         float tail = p3;
         if (r.z == r.w) { tail += p2; if (r.y == r.w) { tail += p1; if (r.x == r.w) tail += p0; } }
