@@ -176,24 +176,45 @@ int Engine::add_csr(const csr_matrix_if& c, int method)
             return rc;
     }
     if (method == 2) {
-        // row blocks: <= kAdaptNnz entries and <= kAdaptThreads rows, or one long row
-        std::vector<int> blocks;
-        blocks.push_back(0);
+        // work blocks: chunks of long rows first, then runs of whole rows
+        std::vector<int4> chunks, runs, longs;
+        int nslots = 0;
         int r = 0;
+        const int* rp = c.csr_row_ptr;
         while (r < m) {
+            const int len = rp[r + 1] - rp[r];
+            if (len > dev::kAdaptNnz) {
+                const int lid = (int)longs.size();
+                const int nch = (len + dev::kAdaptNnz - 1) / dev::kAdaptNnz;
+                longs.push_back(make_int4(r, nslots, nch, 0));
+                for (int k = 0; k < nch; k++)
+                    chunks.push_back(make_int4(k, -(lid + 1), rp[r] + k * dev::kAdaptNnz,
+                                               std::min(rp[r] + (k + 1) * dev::kAdaptNnz, rp[r + 1])));
+                nslots += nch;
+                r++;
+                continue;
+            }
             const int start = r;
             long long acc = 0;
             while (r < m && r - start < dev::kAdaptThreads) {
-                const int len = c.csr_row_ptr[r + 1] - c.csr_row_ptr[r];
-                if (acc + len > dev::kAdaptNnz) break;
-                acc += len;
+                const int l = rp[r + 1] - rp[r];
+                if (l > dev::kAdaptNnz || acc + l > dev::kAdaptNnz) break;
+                acc += l;
                 r++;
             }
-            if (r == start) r++;   // a row longer than the budget forms its own block
-            blocks.push_back(r);
+            runs.push_back(make_int4(start, r - start, rp[start], rp[r]));
         }
-        p.nblocks = (int)blocks.size() - 1;
-        if ((rc = upload_int(&p.i2, blocks.data(), blocks.size(), blocks.size()))) return rc;
+        std::vector<int4> blocks(chunks);
+        blocks.insert(blocks.end(), runs.begin(), runs.end());
+        p.nblocks = (int)blocks.size();
+        if ((rc = alloc(reinterpret_cast<void**>(&p.blocks), std::max<size_t>(blocks.size(), 1) * sizeof(int4))) ||
+            (rc = alloc(reinterpret_cast<void**>(&p.long_rows), std::max<size_t>(longs.size(), 1) * sizeof(int4))) ||
+            (rc = alloc(reinterpret_cast<void**>(&p.scratch_val), std::max(nslots, 1) * sizeof(float))) ||
+            (rc = alloc(reinterpret_cast<void**>(&p.scratch_row), std::max<size_t>(longs.size(), 1) * sizeof(int))))
+            return rc;
+        if (!blocks.empty()) CSP_CUDA(cudaMemcpy(p.blocks, blocks.data(), blocks.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        if (!longs.empty()) CSP_CUDA(cudaMemcpy(p.long_rows, longs.data(), longs.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        CSP_CUDA(cudaMemset(p.scratch_row, 0, std::max<size_t>(longs.size(), 1) * sizeof(int)));   // arrival counters
     }
     if (method == 3) {
         const double mean = m ? (double)nnz / m : 0.0;
@@ -464,7 +485,8 @@ static void launch_part(const Part& p, const float* x, float* y, int n, cudaStre
         switch (p.method) {
         case 0: csr_vector_kernel<V, 32><<<grid_for((long long)p.m * 32, 256), 256, 0, st>>>(p.i0, p.i1, v, x, y, p.m); break;
         case 1: csr_block_row_kernel<V, 128><<<p.m, 128, 0, st>>>(p.i0, p.i1, v, x, y, p.m); break;
-        case 2: csr_adaptive_kernel<V><<<p.nblocks, kAdaptThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.i2); break;
+        case 2: csr_adaptive_kernel<V><<<p.nblocks, kAdaptThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.blocks, p.long_rows,
+                                                                             p.scratch_val, p.scratch_row); break;
         case 3: {
             const unsigned g = grid_for((long long)p.m * p.group, 256);
             switch (p.group) {

@@ -17,10 +17,11 @@ struct Part {
     int method = 0;
     int* i0 = nullptr;   // row_ptr / slice_ptr / offsets / COO rows
     int* i1 = nullptr;   // col ids / band pointers / COO cols
-    int* i2 = nullptr;   // CSR adaptive row blocks
+    int4* blocks = nullptr;     // CSR adaptive work blocks
+    int4* long_rows = nullptr;  // CSR adaptive long rows {row, first slot, chunks, -}
     void* v = nullptr;   // values (FP32 or BF16)
-    int* scratch_row = nullptr;   // COO chunk heads/tails
-    float* scratch_val = nullptr;
+    int* scratch_row = nullptr;   // COO chunk heads/tails; CSR adaptive arrival counters
+    float* scratch_val = nullptr; // COO partial sums; CSR adaptive long-row partials
     int m = 0;        // rows (or block rows' parent height)
     int nnz = 0;
     int k = 0;        // ELL width / #diagonals / #bands / BELL slots

@@ -121,72 +121,122 @@ __global__ void __launch_bounds__(THREADS) csr_block_row_kernel(const int* __res
 
 // ---------------------------------------------------------------------------
 // CSR adaptive (this library's B200 kernel for irregular rows).  The host cuts the
-// rows into row blocks of at most ADAPT_NNZ entries and at most THREADS rows
-// (a longer row forms a block on its own).  A CTA streams its block's entries with
-// coalesced 128-bit loads into shared memory as products val*x[col], then reduces
-// each row from shared memory with a lane group sized to the block's row count; a
-// single long row is reduced by the whole CTA.  Every row is written by exactly one
-// thread, so the result is deterministic.
+// matrix into work blocks of at most kAdaptNnz entries: runs of whole rows (at most
+// kAdaptThreads of them), or one chunk of a row longer than kAdaptNnz, so every CTA
+// moves about the same bytes.  Each block is described by an int4
+// {first row, row count, first entry, end entry}, or for a chunk
+// {chunk index, -(long row id + 1), first entry, end entry}; chunk blocks come first
+// in the grid.
+//
+// A CTA issues every independent load of its block at once -- the 128-bit column
+// and value vectors (at most two per thread), the block's row pointers and its y
+// values -- then the x gathers, so a block costs two dependent memory round trips.
+// Products go to shared memory; each row is reduced by a lane group sized to the
+// block's row count and written once (y = y + sum).  A chunk of a long row writes
+// its partial sum to a scratch slot; the CTA that finishes a row's last chunk (an
+// integer arrival counter, reset by that CTA for the next SpMV) adds the row's
+// partials in chunk order.  Results are deterministic.
 // ---------------------------------------------------------------------------
 constexpr int kAdaptThreads = 256;
-constexpr int kAdaptNnz = 2048;
+constexpr int kAdaptNnz = 2040;                      // <= 2 aligned 4-vectors per thread
+constexpr int kAdaptVecs = (kAdaptNnz + 3) / 4 + 1;  // 511
 
 template <int G>
-__device__ __forceinline__ void adaptive_rows(const int* __restrict__ rp, const float* prod, int s4, int r0, int r1,
+__device__ __forceinline__ void adaptive_rows(const int* s_rp, const float* prod, const float* s_y, int r0, int nrows,
                                               float* __restrict__ y)
 {
     const int lane = threadIdx.x % G;
     const int ngroups = kAdaptThreads / G;
     // uniform trip count across the CTA so every lane takes part in the shuffles
-    for (int first = r0; first < r1; first += ngroups) {
-        const int r = first + threadIdx.x / G;
-        const bool valid = r < r1;
-        const int a = valid ? __ldg(rp + r) - s4 : 0, b = valid ? __ldg(rp + r + 1) - s4 : 0;
+    for (int first = 0; first < nrows; first += ngroups) {
+        const int lr = first + threadIdx.x / G;
+        const bool valid = lr < nrows;
+        const int a = valid ? s_rp[lr] : 0, b = valid ? s_rp[lr + 1] : 0;
         float acc = 0.0f;
         for (int j = a + lane; j < b; j += G) acc += prod[j];
         acc = group_sum<G>(acc);
-        if (valid && lane == 0) y[r] += acc;
+        if (valid && lane == 0) y[r0 + lr] = s_y[lr] + acc;
     }
 }
 
 template <class V>
 __global__ void __launch_bounds__(kAdaptThreads) csr_adaptive_kernel(const int* __restrict__ rp, const int* __restrict__ col,
                                                                      const V* __restrict__ val, const float* __restrict__ x,
-                                                                     float* __restrict__ y, const int* __restrict__ blocks)
+                                                                     float* __restrict__ y, const int4* __restrict__ blocks,
+                                                                     const int4* __restrict__ long_rows,
+                                                                     float* __restrict__ partial, int* __restrict__ arrivals)
 {
-    __shared__ __align__(16) float prod[kAdaptNnz + 8];
+    __shared__ __align__(16) float prod[4 * kAdaptVecs];
+    __shared__ int s_rp[kAdaptThreads + 1];
+    __shared__ float s_y[kAdaptThreads];
     __shared__ float red[kAdaptThreads / 32];
-    const int r0 = __ldg(blocks + blockIdx.x), r1 = __ldg(blocks + blockIdx.x + 1);
-    const int s = __ldg(rp + r0), e = __ldg(rp + r1);
-    if (e - s > kAdaptNnz) {
-        // one long row
-        float acc = segment_dot<V, kAdaptThreads>(col, val, x, s, e, threadIdx.x);
-        acc = block_sum(acc, red);
-        if (threadIdx.x == 0) y[r0] += acc;
+    __shared__ bool s_last;
+    const int4 blk = __ldg(blocks + blockIdx.x);
+    const int r0 = blk.x, code = blk.y, s = blk.z, e = blk.w;
+    const int s4 = s & ~3;
+    const int nvec = (e - s4 + 3) >> 2;
+    const int tid = threadIdx.x;
+
+    // --- every independent load first ---
+    const int v0 = tid, v1 = tid + kAdaptThreads;
+    int4 c0 = make_int4(0, 0, 0, 0), c1 = c0;
+    float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0;
+    if (v0 < nvec) { c0 = ld_int4(col + s4 + 4 * v0); a0 = Val<V>::ld4(val + s4 + 4 * v0); }
+    if (v1 < nvec) { c1 = ld_int4(col + s4 + 4 * v1); a1 = Val<V>::ld4(val + s4 + 4 * v1); }
+    const int nrows = code > 0 ? code : 1;
+    if (code > 0) {
+        // nrows can equal the CTA width, so the end pointer (= e) is written separately
+        if (tid < nrows) s_rp[tid] = __ldg(rp + r0 + tid) - s4;
+        if (tid == 0) s_rp[nrows] = e - s4;
+        if (tid < nrows) s_y[tid] = y[r0 + tid];
+    }
+    // --- dependent x gathers; entries outside [s, e) contribute nothing ---
+    float4 p0, p1;
+    {
+        const int j = s4 + 4 * v0;
+        p0.x = (j + 0 >= s && j + 0 < e) ? a0.x * ldx(x, c0.x) : 0.0f;
+        p0.y = (j + 1 >= s && j + 1 < e) ? a0.y * ldx(x, c0.y) : 0.0f;
+        p0.z = (j + 2 >= s && j + 2 < e) ? a0.z * ldx(x, c0.z) : 0.0f;
+        p0.w = (j + 3 >= s && j + 3 < e) ? a0.w * ldx(x, c0.w) : 0.0f;
+    }
+    {
+        const int j = s4 + 4 * v1;
+        p1.x = (j + 0 >= s && j + 0 < e) ? a1.x * ldx(x, c1.x) : 0.0f;
+        p1.y = (j + 1 >= s && j + 1 < e) ? a1.y * ldx(x, c1.y) : 0.0f;
+        p1.z = (j + 2 >= s && j + 2 < e) ? a1.z * ldx(x, c1.z) : 0.0f;
+        p1.w = (j + 3 >= s && j + 3 < e) ? a1.w * ldx(x, c1.w) : 0.0f;
+    }
+    if (code < 0) {
+        // one chunk of a long row: CTA-wide sum to a scratch slot
+        float t = (p0.x + p0.y) + (p0.z + p0.w) + ((p1.x + p1.y) + (p1.z + p1.w));
+        t = block_sum(t, red);
+        const int4 lr = __ldg(long_rows + (-code - 1));   // {row, first slot, chunks, -}
+        const int chunk = r0;                              // a chunk block carries its chunk index here
+        if (tid == 0) {
+            partial[lr.y + chunk] = t;
+            __threadfence();
+            const int seen = atomicAdd(arrivals + (-code - 1), 1);
+            s_last = (seen == lr.z - 1);
+        }
+        __syncthreads();
+        if (s_last && tid == 0) {
+            __threadfence();
+            float tot = 0.0f;
+            for (int k = 0; k < lr.z; k++) tot += __ldcg(partial + lr.y + k);
+            y[lr.x] += tot;
+            arrivals[-code - 1] = 0;
+        }
         return;
     }
-    const int s4 = s & ~3;
-    const int nvec = (e - s4 + 3) >> 2;   // <= kAdaptNnz / 4 + 1
-    for (int v = threadIdx.x; v < nvec; v += kAdaptThreads) {
-        const int j = s4 + 4 * v;
-        const int4 c = ld_int4(col + j);
-        const float4 a = Val<V>::ld4(val + j);
-        float4 p;
-        p.x = (j + 0 >= s && j + 0 < e) ? a.x * ldx(x, c.x) : 0.0f;
-        p.y = (j + 1 >= s && j + 1 < e) ? a.y * ldx(x, c.y) : 0.0f;
-        p.z = (j + 2 >= s && j + 2 < e) ? a.z * ldx(x, c.z) : 0.0f;
-        p.w = (j + 3 >= s && j + 3 < e) ? a.w * ldx(x, c.w) : 0.0f;
-        reinterpret_cast<float4*>(prod)[v] = p;
-    }
+    if (v0 < nvec) reinterpret_cast<float4*>(prod)[v0] = p0;
+    if (v1 < nvec) reinterpret_cast<float4*>(prod)[v1] = p1;
     __syncthreads();
-    const int nrows = r1 - r0;
-    // lanes per row: as many as the block's row count allows, at most a warp
-    if (nrows * 32 <= kAdaptThreads) adaptive_rows<32>(rp, prod, s4, r0, r1, y);
-    else if (nrows * 16 <= kAdaptThreads) adaptive_rows<16>(rp, prod, s4, r0, r1, y);
-    else if (nrows * 8 <= kAdaptThreads) adaptive_rows<8>(rp, prod, s4, r0, r1, y);
-    else if (nrows * 4 <= kAdaptThreads) adaptive_rows<4>(rp, prod, s4, r0, r1, y);
-    else if (nrows * 2 <= kAdaptThreads) adaptive_rows<2>(rp, prod, s4, r0, r1, y);
-    else adaptive_rows<1>(rp, prod, s4, r0, r1, y);
+    if (nrows * 32 <= kAdaptThreads) adaptive_rows<32>(s_rp, prod, s_y, r0, nrows, y);
+    else if (nrows * 16 <= kAdaptThreads) adaptive_rows<16>(s_rp, prod, s_y, r0, nrows, y);
+    else if (nrows * 8 <= kAdaptThreads) adaptive_rows<8>(s_rp, prod, s_y, r0, nrows, y);
+    else if (nrows * 4 <= kAdaptThreads) adaptive_rows<4>(s_rp, prod, s_y, r0, nrows, y);
+    else if (nrows * 2 <= kAdaptThreads) adaptive_rows<2>(s_rp, prod, s_y, r0, nrows, y);
+    else adaptive_rows<1>(s_rp, prod, s_y, r0, nrows, y);
 }
 
 // ---------------------------------------------------------------------------
@@ -221,11 +271,21 @@ __global__ void __launch_bounds__(256) coo_segment_kernel(const int* __restrict_
     int carry_row = head_row;
     float carry_val = 0.0f;
 
+    // software pipeline: the next tile's rows, columns and values are in flight while
+    // the current tile gathers x and reduces
+    int4 rn = ld_int4(rowid + base + 4 * lane);
+    int4 cn = ld_int4(colid + base + 4 * lane);
+    float4 an = Val<V>::ld4(val + base + 4 * lane);
     for (int t = base; t < end; t += 128) {
-        const int j = t + 4 * lane;
-        const int4 r = ld_int4(rowid + j);
-        const int4 c = ld_int4(colid + j);
-        const float4 a = Val<V>::ld4(val + j);
+        const int4 r = rn;
+        const int4 c = cn;
+        const float4 a = an;
+        if (t + 128 < end) {
+            const int jn = t + 128 + 4 * lane;
+            rn = ld_int4(rowid + jn);
+            cn = ld_int4(colid + jn);
+            an = Val<V>::ld4(val + jn);
+        }
         const float p0 = a.x * ldx(x, c.x), p1 = a.y * ldx(x, c.y);
         const float p2 = a.z * ldx(x, c.z), p3 = a.w * ldx(x, c.w);
         // the segment carried out of the previous tile ends if this tile starts a new row

@@ -10,7 +10,20 @@ from tests.gpu_util import check, coo_of, run, vecs
 pytestmark = pytest.mark.gpu
 
 CASES = small_cases()
+def _long_rows(seed=24):
+    """A few very long rows among short ones: 3 rows of 150,000 entries in 2,000 x 200,000."""
+    rng = np.random.default_rng(seed)
+    h, w = 2000, 200_000
+    lens = rng.integers(0, 9, h)
+    lens[[0, 777, 1999]] = 150_000
+    rows = np.repeat(np.arange(h), lens)
+    cols = np.concatenate([np.sort(rng.choice(w, k, replace=False)) for k in lens])
+    vals = rng.standard_normal(rows.size).astype(np.float32)
+    return h, w, rows.astype(np.int32), cols.astype(np.int32), vals
+
+
 MEDIUM = {
+    "long_rows": _long_rows(),
     "zipf_100k": M.zipf_rows(100_000, seed=21, max_len=6000),
     "stencil24": M.stencil_27(24, seed=22),
     "block3_5k": M.block_3x3(5000, deg=(10, 30), band=300, seed=23),
@@ -42,8 +55,10 @@ def test_flat_and_block(name, variant):
     fmt, method, kw = variant
     case = ALL[name]
     h, w = case[0], case[1]
-    if fmt in ("bell", "sbell", "bcsr") and name in ("zipf_100k",) and kw.get("bheight", 1) * kw.get("bwidth", 4) > 8:
+    if fmt in ("bell", "sbell", "bcsr") and name in ("zipf_100k", "long_rows") and kw.get("bheight", 1) * kw.get("bwidth", 4) > 8:
         pytest.skip("block padding of a random matrix exceeds the memory-object limit")
+    if fmt in ("ell", "bell") and name == "long_rows":
+        pytest.skip("ELL padding of 150,000-entry rows: 1.2 GB of zeros")
     try:
         mat = Cocktail.single(fmt, coo_of(case), method, **kw)
     except Exception as e:  # the reference refuses some block shapes (MAX_MEM_OBJ)
