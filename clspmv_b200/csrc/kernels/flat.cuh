@@ -286,6 +286,11 @@ __global__ void __launch_bounds__(256) coo_segment_kernel(const int* __restrict_
             cn = ld_int4(colid + jn);
             an = Val<V>::ld4(val + jn);
         }
+        // y of the tile's rows is requested together with the x gathers, so closing a
+        // segment needs no further round trip.  A row closed here is written only by the
+        // lane that closes it (head and tail rows go to the scratch pairs instead), so
+        // the value read is still the original y.
+        const float y0 = y[r.x], y1 = y[r.y], y2 = y[r.z], y3 = y[r.w];
         const float p0 = a.x * ldx(x, c.x), p1 = a.y * ldx(x, c.y);
         const float p2 = a.z * ldx(x, c.z), p3 = a.w * ldx(x, c.w);
         // the segment carried out of the previous tile ends if this tile starts a new row
@@ -324,6 +329,7 @@ __global__ void __launch_bounds__(256) coo_segment_kernel(const int* __restrict_
         // walk the lane's four entries, closing segments
         const int rr[4] = {r.x, r.y, r.z, r.w};
         const float pp[4] = {p0, p1, p2, p3};
+        const float yy[4] = {y0, y1, y2, y3};
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             run += pp[k];
@@ -336,7 +342,7 @@ __global__ void __launch_bounds__(256) coo_segment_kernel(const int* __restrict_
                     part_val[2 * w] = run;
                     closed_head = true;
                 } else {
-                    y[rr[k]] += run;
+                    y[rr[k]] = yy[k] + run;
                 }
                 run = 0.0f;
             }
