@@ -21,6 +21,7 @@ FP = C.POINTER(C.c_float)
 CSP_OK, CSP_EINVAL, CSP_ENOMEM, CSP_ECUDA, CSP_EFORMAT, CSP_ENODEV, CSP_EUNSUP, CSP_EIO, CSP_ETIMEOUT = range(9)
 CSP_FLAG_USE_TEX, CSP_FLAG_BF16, CSP_FLAG_GRAPH, CSP_FLAG_ADJOINT = 0x1, 0x2, 0x4, 0x8
 CSP_ANALYZE_REFERENCE, CSP_ANALYZE_AUTOTUNE = 0, 1
+CSP_NOALLOC_MAX_NNZ = 33554432
 
 
 class matrixInfo(C.Structure):
@@ -192,6 +193,8 @@ def _declare(lib):
         "csp_evaluate": (C.c_int, [P(cocktail), FP, FP, FP, C.c_int, P(csp_report)]),
         "csp_spmv_all": (C.c_int, [P(coo_matrix), C.c_int, C.c_int, P(csp_report)]),
         "csp_read_mmf": (C.c_int, [C.c_char_p, P(coo_matrix)]),
+        "csp_coo_spmv_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -364,6 +364,30 @@ int csp_spmv_bcsr(coo_matrix_if* coo, int ntimes, csp_report* report);
 int csp_spmv_sbell(coo_matrix_if* coo, int ntimes, csp_report* report);
 
 /* ------------------------------------------------------------------------ */
+/* SpMV without device allocation.  No counterpart in the reference.          */
+/*                                                                            */
+/* For callers that cannot allocate device memory -- code running under a     */
+/* framework allocator that already owns the device, real-time loops where    */
+/* cudaMalloc/cudaFree (which may synchronize the device) are forbidden,      */
+/* embedders that pass only buffers they own.  Computes y += A*x for a COO    */
+/* matrix held by the caller in device memory (rows sorted, 16-byte aligned   */
+/* arrays), on `stream` (NULL = legacy default stream), allocating nothing:   */
+/* its scratch is a fixed 1 MiB array inside this library's device image,     */
+/* held by every GPU that loads the library until the process exits, which    */
+/* limits nnz to CSP_NOALLOC_MAX_NNZ (larger matrices: CSP_EINVAL).           */
+/* The first call on each device looks the array's address up for that       */
+/* device, so make it before capturing the call into a CUDA graph.  All calls */
+/* on a device share the array: calls that overlap on the GPU (other streams, */
+/* other host threads) race and must be serialized by the caller.  Nothing in */
+/* the array needs clearing between calls: each call writes every slot it     */
+/* reads.  Out-of-range row or column ids are skipped, not dereferenced.      */
+/* ------------------------------------------------------------------------ */
+#define CSP_NOALLOC_MAX_NNZ       33554432   /* 2^25 entries                          */
+#define CSP_NOALLOC_SCRATCH_BYTES 1048576    /* 2 (row, partial) pairs per 512 entries */
+int csp_coo_spmv_noalloc(int height, int width, int nnz, const int* d_row, const int* d_col, const float* d_val,
+                         const float* d_x, float* d_y, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* MatrixMarket input (fileio.cpp:10 ReadMMF): 0-based, pattern -> 1.0,       */
 /* symmetric mirrored, sorted.                                               */
 /* ------------------------------------------------------------------------ */
