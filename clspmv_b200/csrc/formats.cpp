@@ -72,7 +72,7 @@ static void row_pointer(const coo_matrix_if* s, std::vector<int>& rp)
 // (matrix_storage.h:745-815: middle element as pivot, moved to the left end first;
 // at most kMaxLevels pending ranges, else failure).  Reproducing the steps keeps the
 // order of duplicate (row, col) entries identical to the reference's.
-static bool quicksort_coo(int* row, int* col, float* val, int n)
+bool quicksort_coo(int* row, int* col, float* val, int n)
 {
     std::vector<int> lo(kMaxLevels), hi(kMaxLevels);
     int depth = 0;
@@ -133,15 +133,9 @@ int ensure_sorted(coo_matrix_if* m)
 // Blocks of one block row, in the reference's order (matrix_storage.h:1631-1697): the
 // entries of bheight rows sorted by (col, row), grouped into blocks whose column is
 // col - col % bwidth; each block's bwidth*bheight values row-major, later duplicates win.
-struct BlockRows {
-    std::vector<int> rowptr;   // per block row
-    std::vector<int> colid;    // block column (original column units)
-    std::vector<float> data;   // blocksize values per block
-};
-
 struct Elem { int rowid; int colid; float data; };
 
-static void build_blocks(const coo_matrix_if* s, unsigned bw, unsigned bh, BlockRows& out)
+void build_blocks(const coo_matrix_if* s, unsigned bw, unsigned bh, BlockRows& out)
 {
     std::vector<int> rp;
     row_pointer(s, rp);
@@ -185,6 +179,109 @@ static void build_blocks(const coo_matrix_if* s, unsigned bw, unsigned bh, Block
         }
         out.rowptr[br + 1] = out.rowptr[br] + nblocks;
     }
+}
+
+// b4csr layout (matrix_storage.h:1741-1897 coo2b4csr; analyze.cpp:2113 extract_bcsr_part):
+// column ids /4; data [w4 * (al * bh) + h * al + blk * 4 + w], al = aligned_length(4 * #blocks).
+int write_b4csr(const BlockRows& b, unsigned bw, unsigned bh, int alignment, b4csr_matrix_if* d)
+{
+    const long long nb = (long long)b.colid.size();
+    const unsigned bs = bw * bh, bw4 = bw / 4;
+    const int al = csp_aligned_length((int)nb * 4, alignment);
+    d->b4csr_bwidth = bw;
+    d->b4csr_bheight = bh;
+    d->b4csr_row_num = (int)b.rowptr.size() - 1;
+    d->b4csr_aligned_size = al;
+    d->b4csr_block_num = (int)nb;
+    d->b4csr_row_ptr = xmalloc<int>(b.rowptr.size());
+    d->b4csr_col_id = xmalloc<int>((size_t)nb);
+    d->b4csr_data = xcalloc<float>((size_t)al * bh * bw4);
+    if (!d->b4csr_row_ptr || !d->b4csr_col_id || !d->b4csr_data) return set_error(CSP_ENOMEM, "b4csr layout");
+    memcpy(d->b4csr_row_ptr, b.rowptr.data(), b.rowptr.size() * sizeof(int));
+    const size_t rowlen = (size_t)al * bh;
+    for (long long i = 0; i < nb; i++) {
+        d->b4csr_col_id[i] = b.colid[i] / 4;
+        for (unsigned h = 0; h < bh; h++)
+            for (unsigned w4 = 0; w4 < bw4; w4++)
+                for (unsigned w = 0; w < 4; w++)
+                    d->b4csr_data[w4 * rowlen + (size_t)h * al + (size_t)i * 4 + w] =
+                        b.data[(size_t)i * bs + h * bw + w4 * 4 + w];
+    }
+    return CSP_OK;
+}
+
+// b4ell layout (matrix_storage.h:2010-2200 coo2b4ell; analyze.cpp:1888 extract_bell_part):
+// `ellnum` slots per block row; short rows repeat their last block column, zero data.
+int write_b4ell(const BlockRows& b, unsigned bw, unsigned bh, int alignment, int ellnum, b4ell_matrix_if* d)
+{
+    const int nbr = (int)b.rowptr.size() - 1;
+    const unsigned bs = bw * bh, bw4 = bw / 4;
+    const int hal = csp_aligned_length(nbr, alignment);
+    const int f4 = csp_aligned_length(4 * nbr, alignment);
+    d->b4ell_bwidth = bw;
+    d->b4ell_bheight = bh;
+    d->b4ell_row_num = nbr;
+    d->b4ell_block_num = ellnum;
+    d->b4ell_height_aligned = hal;
+    d->b4ell_float4_aligned = f4;
+    d->b4ell_col_id = xcalloc<int>((size_t)hal * ellnum);
+    d->b4ell_data = xcalloc<float>((size_t)f4 * bh * bw4 * ellnum);
+    if (!d->b4ell_col_id || !d->b4ell_data) return set_error(CSP_ENOMEM, "b4ell layout");
+    const size_t colsize = (size_t)f4 * bw4 * bh, w4size = (size_t)f4 * bh;
+    for (int r = 0; r < nbr; r++) {
+        int last = 0, k = 0;
+        for (int j = b.rowptr[r]; j < b.rowptr[r + 1]; j++, k++) {
+            d->b4ell_col_id[r + (size_t)k * hal] = last = b.colid[j] / 4;
+            for (unsigned h = 0; h < bh; h++)
+                for (unsigned w4 = 0; w4 < bw4; w4++)
+                    for (unsigned w = 0; w < 4; w++)
+                        d->b4ell_data[(size_t)k * colsize + (size_t)h * f4 + w4 * w4size + (size_t)r * 4 + w] =
+                            b.data[(size_t)j * bs + h * bw + w4 * 4 + w];
+        }
+        for (; k < ellnum; k++) d->b4ell_col_id[r + (size_t)k * hal] = last;
+    }
+    return CSP_OK;
+}
+
+// sbell layout (matrix_storage.h:2203-2409 coo2sbell; analyze.cpp:1660 extract_sbell_part):
+// slice i holds width[i] slots for each of its `sh` block rows.
+int write_sbell(const BlockRows& b, unsigned bw, unsigned bh, unsigned sh, const std::vector<int>& width,
+                sbell_matrix_if* d)
+{
+    const int nbr = (int)b.rowptr.size() - 1;
+    const int H = (int)sh;
+    const int nslices = (int)width.size();
+    d->sbell_bwidth = bw;
+    d->sbell_bheight = bh;
+    d->sbell_slice_num = nslices;
+    d->sbell_row_num = nbr;
+    d->sbell_slice_height = sh;
+    d->sbell_slice_ptr = xmalloc<int>((size_t)nslices + 1);
+    if (!d->sbell_slice_ptr) return set_error(CSP_ENOMEM, "sbell layout");
+    d->sbell_slice_ptr[0] = 0;
+    for (int i = 0; i < nslices; i++) d->sbell_slice_ptr[i + 1] = d->sbell_slice_ptr[i] + width[i] * H;
+    const long long total = d->sbell_slice_ptr[nslices];
+    const unsigned bs = bw * bh, bw4 = bw / 4;
+    d->sbell_col_id = xcalloc<int>((size_t)total);
+    d->sbell_data = xcalloc<float>((size_t)total * bs);
+    if (!d->sbell_col_id || !d->sbell_data) return set_error(CSP_ENOMEM, "sbell layout");
+    const size_t colsize = (size_t)H * bw4 * bh * 4, w4size = (size_t)H * bh * 4, hsize = (size_t)H * 4;
+    for (int r = 0; r < nbr; r++) {
+        const int sl = r / H, lr = r % H;
+        const size_t cstart = (size_t)d->sbell_slice_ptr[sl];
+        const size_t dstart = cstart * bs;
+        int last = 0, k = 0;
+        for (int j = b.rowptr[r]; j < b.rowptr[r + 1]; j++, k++) {
+            d->sbell_col_id[cstart + lr + (size_t)k * H] = last = b.colid[j] / 4;
+            for (unsigned h = 0; h < bh; h++)
+                for (unsigned w4 = 0; w4 < bw4; w4++)
+                    for (unsigned w = 0; w < 4; w++)
+                        d->sbell_data[dstart + (size_t)k * colsize + h * hsize + w4 * w4size + (size_t)lr * 4 + w] =
+                            b.data[(size_t)j * bs + h * bw + w4 * 4 + w];
+        }
+        for (; k < width[sl]; k++) d->sbell_col_id[cstart + lr + (size_t)k * H] = last;
+    }
+    return CSP_OK;
 }
 
 }  // namespace csp
@@ -647,26 +744,7 @@ int csp_coo2b4csr(coo_matrix_if* s, b4csr_matrix_if* d, unsigned bw, unsigned bh
     const long long nb = (long long)b.colid.size();
     if (nb > kMaxMemObj / (long long)(bw * bh * sizeof(float)))
         return set_error(CSP_EFORMAT, "coo2b4csr: %lld blocks exceed the memory-object limit", nb);
-    const unsigned bs = bw * bh, bw4 = bw / 4;
-    const int al = csp_aligned_length((int)nb * 4, alignment);
-    d->b4csr_row_num = (int)b.rowptr.size() - 1;
-    d->b4csr_aligned_size = al;
-    d->b4csr_block_num = (int)nb;
-    d->b4csr_row_ptr = xmalloc<int>(b.rowptr.size());
-    d->b4csr_col_id = xmalloc<int>((size_t)nb);
-    d->b4csr_data = xcalloc<float>((size_t)al * bh * bw4);
-    if (!d->b4csr_row_ptr || !d->b4csr_col_id || !d->b4csr_data) return set_error(CSP_ENOMEM, "coo2b4csr");
-    memcpy(d->b4csr_row_ptr, b.rowptr.data(), b.rowptr.size() * sizeof(int));
-    const size_t rowlen = (size_t)al * bh;
-    for (long long i = 0; i < nb; i++) {
-        d->b4csr_col_id[i] = b.colid[i] / 4;
-        for (unsigned h = 0; h < bh; h++)
-            for (unsigned w4 = 0; w4 < bw4; w4++)
-                for (unsigned w = 0; w < 4; w++)
-                    d->b4csr_data[w4 * rowlen + (size_t)h * al + (size_t)i * 4 + w] =
-                        b.data[(size_t)i * bs + h * bw + w4 * 4 + w];
-    }
-    return CSP_OK;
+    return write_b4csr(b, bw, bh, alignment, d);
 }
 
 // matrix_storage.h:2010 coo2b4ell: block ELL in the b4 layout.  Column ids (float4
@@ -690,30 +768,7 @@ int csp_coo2b4ell(coo_matrix_if* s, b4ell_matrix_if* d, unsigned bw, unsigned bh
     if (ellnum < maxw) return set_error(CSP_EINVAL, "coo2b4ell: ellnum below the widest block row");
     if ((long long)nbr * ellnum > kMaxMemObj / (long long)(bw * bh * sizeof(float)))
         return set_error(CSP_EFORMAT, "coo2b4ell: exceeds the memory-object limit");
-    const unsigned bs = bw * bh, bw4 = bw / 4;
-    const int hal = csp_aligned_length(nbr, alignment);
-    const int f4 = csp_aligned_length(4 * nbr, alignment);
-    d->b4ell_row_num = nbr;
-    d->b4ell_block_num = ellnum;
-    d->b4ell_height_aligned = hal;
-    d->b4ell_float4_aligned = f4;
-    d->b4ell_col_id = xcalloc<int>((size_t)hal * ellnum);
-    d->b4ell_data = xcalloc<float>((size_t)f4 * bh * bw4 * ellnum);
-    if (!d->b4ell_col_id || !d->b4ell_data) return set_error(CSP_ENOMEM, "coo2b4ell");
-    const size_t colsize = (size_t)f4 * bw4 * bh, w4size = (size_t)f4 * bh;
-    for (int r = 0; r < nbr; r++) {
-        int last = 0, k = 0;
-        for (int j = b.rowptr[r]; j < b.rowptr[r + 1]; j++, k++) {
-            d->b4ell_col_id[r + (size_t)k * hal] = last = b.colid[j] / 4;
-            for (unsigned h = 0; h < bh; h++)
-                for (unsigned w4 = 0; w4 < bw4; w4++)
-                    for (unsigned w = 0; w < 4; w++)
-                        d->b4ell_data[(size_t)k * colsize + (size_t)h * f4 + w4 * w4size + (size_t)r * 4 + w] =
-                            b.data[(size_t)j * bs + h * bw + w4 * 4 + w];
-        }
-        for (; k < ellnum; k++) d->b4ell_col_id[r + (size_t)k * hal] = last;
-    }
-    return CSP_OK;
+    return write_b4ell(b, bw, bh, alignment, ellnum, d);
 }
 
 // matrix_storage.h:2203 coo2sbell: sliced b4 block ELL, slices of `sh` block rows, slice
@@ -737,43 +792,17 @@ int csp_coo2sbell(coo_matrix_if* s, sbell_matrix_if* d, unsigned bw, unsigned bh
     d->sbell_slice_num = nslices;
     d->sbell_row_num = nbr;
     d->sbell_slice_height = sh;
-    d->sbell_slice_ptr = xmalloc<int>((size_t)nslices + 1);
-    if (!d->sbell_slice_ptr) return set_error(CSP_ENOMEM, "coo2sbell");
-    d->sbell_slice_ptr[0] = 0;
     std::vector<int> width((size_t)nslices);
+    long long total = 0;
     for (int i = 0; i < nslices; i++) {
         int w = 0;
         for (int r = i * H; r < (i + 1) * H && r < nbr; r++) w = std::max(w, b.rowptr[r + 1] - b.rowptr[r]);
         width[i] = w;
-        d->sbell_slice_ptr[i + 1] = d->sbell_slice_ptr[i] + w * H;
+        total += (long long)w * H;
     }
-    const long long total = d->sbell_slice_ptr[nslices];
-    if (total > kMaxMemObj / (long long)(bw * bh * sizeof(float))) {
-        free(d->sbell_slice_ptr);
-        d->sbell_slice_ptr = nullptr;
+    if (total > kMaxMemObj / (long long)(bw * bh * sizeof(float)))
         return set_error(CSP_EFORMAT, "coo2sbell: exceeds the memory-object limit");
-    }
-    const unsigned bs = bw * bh, bw4 = bw / 4;
-    d->sbell_col_id = xcalloc<int>((size_t)total);
-    d->sbell_data = xcalloc<float>((size_t)total * bs);
-    if (!d->sbell_col_id || !d->sbell_data) return set_error(CSP_ENOMEM, "coo2sbell");
-    const size_t colsize = (size_t)H * bw4 * bh * 4, w4size = (size_t)H * bh * 4, hsize = (size_t)H * 4;
-    for (int r = 0; r < nbr; r++) {
-        const int sl = r / H, lr = r % H;
-        const size_t cstart = (size_t)d->sbell_slice_ptr[sl];
-        const size_t dstart = cstart * bs;
-        int last = 0, k = 0;
-        for (int j = b.rowptr[r]; j < b.rowptr[r + 1]; j++, k++) {
-            d->sbell_col_id[cstart + lr + (size_t)k * H] = last = b.colid[j] / 4;
-            for (unsigned h = 0; h < bh; h++)
-                for (unsigned w4 = 0; w4 < bw4; w4++)
-                    for (unsigned w = 0; w < 4; w++)
-                        d->sbell_data[dstart + (size_t)k * colsize + h * hsize + w4 * w4size + (size_t)lr * 4 + w] =
-                            b.data[(size_t)j * bs + h * bw + w4 * 4 + w];
-        }
-        for (; k < width[sl]; k++) d->sbell_col_id[cstart + lr + (size_t)k * H] = last;
-    }
-    return CSP_OK;
+    return write_sbell(b, bw, bh, sh, width, d);
 }
 
 // util.cpp:31 pad_csr: every row padded to a multiple of `alignment` with the row's last

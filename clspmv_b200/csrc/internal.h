@@ -2,6 +2,7 @@
 #pragma once
 
 #include <stdarg.h>
+#include <vector>
 #include "csp/clspmv.h"
 
 namespace csp {
@@ -11,6 +12,20 @@ int set_error(int code, const char* fmt, ...);
 void clear_error();
 
 int check_coo(const coo_matrix_if* m);
+
+// Blocks of a matrix in the reference's construction order (matrix_storage.h:1631-1697):
+// per block row, entries sorted by (col, row), one block per distinct col - col % bw.
+struct BlockRows {
+    std::vector<int> rowptr;   // per block row
+    std::vector<int> colid;    // block column (original column units)
+    std::vector<float> data;   // bw*bh values per block, row-major
+};
+void build_blocks(const coo_matrix_if* s, unsigned bw, unsigned bh, BlockRows& out);
+int write_b4csr(const BlockRows& b, unsigned bw, unsigned bh, int alignment, b4csr_matrix_if* d);
+int write_b4ell(const BlockRows& b, unsigned bw, unsigned bh, int alignment, int ellnum, b4ell_matrix_if* d);
+int write_sbell(const BlockRows& b, unsigned bw, unsigned bh, unsigned sh, const std::vector<int>& width,
+                sbell_matrix_if* d);
+bool quicksort_coo(int* row, int* col, float* val, int n);
 bool coo_is_sorted(const coo_matrix_if* m);
 int ensure_sorted(coo_matrix_if* m);
 

@@ -74,9 +74,18 @@ def extract(fmt: str, s) -> dict:
         sp = to_numpy(s.sbell_slice_ptr, s.sbell_slice_num + 1, I32)
         n = int(sp[-1])
         bs = s.sbell_bwidth * s.sbell_bheight
-        d.update(bw=s.sbell_bwidth, bh=s.sbell_bheight, sh=s.sbell_slice_height, num=s.sbell_slice_num,
-                 rows=s.sbell_row_num, sp=sp, col=to_numpy(s.sbell_col_id, n, I32),
-                 val=to_numpy(s.sbell_data, n * bs, F32))
+        sh = s.sbell_slice_height
+        col = to_numpy(s.sbell_col_id, n, I32)
+        # column ids of the block rows past sbell_row_num in the last slice are left
+        # uninitialised by the reference analyzer (analyze.cpp:1819): not compared
+        for sl in range(s.sbell_slice_num):
+            first = sl * sh
+            if first + sh > s.sbell_row_num:
+                width = (sp[sl + 1] - sp[sl]) // sh if sh else 0
+                for lr in range(max(s.sbell_row_num - first, 0), sh):
+                    col[sp[sl] + lr + np.arange(width) * sh] = 0
+        d.update(bw=s.sbell_bwidth, bh=s.sbell_bheight, sh=sh, num=s.sbell_slice_num,
+                 rows=s.sbell_row_num, sp=sp, col=col, val=to_numpy(s.sbell_data, n * bs, F32))
     else:
         raise ValueError(fmt)
     return d
