@@ -104,13 +104,16 @@ class Cocktail:
 
 
 def analyze_matrix(coo: COO, mode: int = CSP_ANALYZE_REFERENCE, bench_path: str | None = None,
-                   verbose: int = 0, cache_path: str | None = None) -> Cocktail:
+                   verbose: int = 0, cache_path: str | None = None, flags: int = 0) -> Cocktail:
     """Partition `coo` into per-format sub-matrices (analyze.cpp:3704).  `coo` may be
-    sorted in place, as in the reference."""
+    sorted in place, as in the reference.  mode=CSP_ANALYZE_AUTOTUNE measures candidate
+    partitions on the device instead of predicting from the clSpMV tables."""
     c = Cocktail()
     opts = capi.csp_analyze_opts(mode, bench_path.encode() if bench_path else None, verbose,
-                                 cache_path.encode() if cache_path else None)
+                                 cache_path.encode() if cache_path else None, flags)
     check(lib().csp_analyze_matrix(coo.ref(), c.ref(), C.byref(opts)), "analyze_matrix")
+    if mode == CSP_ANALYZE_AUTOTUNE:
+        c.choice = lib().csp_autotune_choice().decode()
     return c
 
 

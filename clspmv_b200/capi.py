@@ -99,7 +99,8 @@ class cocktail(C.Structure):
 
 
 class csp_analyze_opts(C.Structure):
-    _fields_ = [("mode", C.c_int), ("bench_path", C.c_char_p), ("verbose", C.c_int), ("cache_path", C.c_char_p)]
+    _fields_ = [("mode", C.c_int), ("bench_path", C.c_char_p), ("verbose", C.c_int), ("cache_path", C.c_char_p),
+                ("flags", C.c_int)]
 
 
 class csp_report(C.Structure):
@@ -193,6 +194,7 @@ def _declare(lib):
         "csp_evaluate": (C.c_int, [P(cocktail), FP, FP, FP, C.c_int, P(csp_report)]),
         "csp_spmv_all": (C.c_int, [P(coo_matrix), C.c_int, C.c_int, P(csp_report)]),
         "csp_read_mmf": (C.c_int, [C.c_char_p, P(coo_matrix)]),
+        "csp_autotune_choice": (C.c_char_p, []),
         "csp_coo_spmv_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p]),
     }

@@ -1304,6 +1304,11 @@ extern "C" int csp_analyze_matrix(coo_matrix_if* coo, cocktail_iif* mat, const c
         mat->mat_nnz = coo->matinfo.nnz;
         return CSP_OK;
     }
+    if (opts && opts->mode == CSP_ANALYZE_AUTOTUNE) {
+        csp_init_cocktail(mat);
+        return autotune_partition(coo, mat, opts);
+    }
+    if (opts && opts->mode != CSP_ANALYZE_REFERENCE) return set_error(CSP_EINVAL, "unknown analyze mode %d", opts->mode);
     const char* path = (opts && opts->bench_path) ? opts->bench_path : getenv("CLSPMVPATH");
     if (!path) return set_error(CSP_EINVAL, "no calibration tables: set CLSPMVPATH or csp_analyze_opts.bench_path");
     ana::Tables t;

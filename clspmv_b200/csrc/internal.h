@@ -27,6 +27,7 @@ int write_sbell(const BlockRows& b, unsigned bw, unsigned bh, unsigned sh, const
                 sbell_matrix_if* d);
 bool quicksort_coo(int* row, int* col, float* val, int n);
 bool coo_is_sorted(const coo_matrix_if* m);
+int autotune_partition(coo_matrix_if* coo, cocktail_iif* out, const csp_analyze_opts* opts);
 int ensure_sorted(coo_matrix_if* m);
 
 }  // namespace csp

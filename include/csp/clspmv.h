@@ -281,15 +281,25 @@ int csp_pad_csr(const csr_matrix_if* src, csr_matrix_if* dst, int alignment);   
 
 typedef struct csp_analyze_opts {
     int mode;                /* CSP_ANALYZE_REFERENCE or CSP_ANALYZE_AUTOTUNE            */
-    const char* bench_path;  /* directory holding benchmark/ *.ben; NULL = $CLSPMVPATH     */
-    int verbose;             /* 0 = silent, 1 = print the reference's progress lines     */
+    const char* bench_path;  /* REFERENCE: directory holding benchmark/ *.ben; NULL = $CLSPMVPATH */
+    int verbose;             /* AUTOTUNE: 1 = print each candidate's measured time        */
     const char* cache_path;  /* AUTOTUNE: file caching decisions per sparsity signature  */
+    int flags;               /* AUTOTUNE: engine flags the partition is tuned for (CSP_FLAG_BF16) */
 } csp_analyze_opts;
 
 /* Partition `coo` into the per-format sub-matrices of `mat`.  `coo` may be
  * sorted in place (as the reference does).  opts may be NULL (REFERENCE mode,
- * $CLSPMVPATH, silent). */
+ * $CLSPMVPATH).
+ * REFERENCE: the reference partition, bit for bit, from the clSpMV tables.
+ * AUTOTUNE: needs a CUDA device; builds candidate partitions (each format and
+ * kernel variant, slice heights 32/128, the eight b4 block shapes, ELL + CSR
+ * splits), times each on the device with L2 flushed between SpMVs, keeps the
+ * fastest, and records the choice under a hash of the sparsity pattern in
+ * cache_path (if given) so the next call on the same pattern skips timing. */
 int csp_analyze_matrix(coo_matrix_if* coo, cocktail_iif* mat, const csp_analyze_opts* opts);
+/* Name of the partition the last AUTOTUNE call on this thread chose ("" if none),
+ * e.g. "csr2", "ell1+csr2", "bcsr4x4m0". */
+const char* csp_autotune_choice(void);
 
 /* ------------------------------------------------------------------------ */
 /* Device engine (spmv_cocktail.h:111-175)                                   */
