@@ -193,6 +193,21 @@ class Handle:
         check(lib().csp_device_bytes(self.h, C.byref(n)), "device_bytes")
         return n.value
 
+    # --- adjoint (handle built with CSP_FLAG_ADJOINT) ---
+    def spmv_adjoint(self, ybar_ptr: int, xbar_ptr: int | None = None, abar_ptr: int | None = None):
+        """xbar += A^T ybar and abar = ybar[row] * x[col] per stored slot (device pointers)."""
+        check(lib().csp_spmv_adjoint(self.h, C.c_void_p(ybar_ptr), C.c_void_p(xbar_ptr) if xbar_ptr else None,
+                                     C.c_void_p(abar_ptr) if abar_ptr else None), "spmv_adjoint")
+
+    @property
+    def adjoint_slots(self) -> int:
+        n = C.c_size_t()
+        check(lib().csp_adjoint_slots(self.h, C.byref(n)), "adjoint_slots")
+        return n.value
+
+    def adjoint_pattern(self, rows_ptr: int, cols_ptr: int):
+        check(lib().csp_adjoint_pattern(self.h, C.c_void_p(rows_ptr), C.c_void_p(cols_ptr)), "adjoint_pattern")
+
     def free(self):
         if self.h:
             lib().csp_free_mat_kernels(self.h)

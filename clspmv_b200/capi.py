@@ -195,6 +195,9 @@ def _declare(lib):
         "csp_spmv_all": (C.c_int, [P(coo_matrix), C.c_int, C.c_int, P(csp_report)]),
         "csp_read_mmf": (C.c_int, [C.c_char_p, P(coo_matrix)]),
         "csp_autotune_choice": (C.c_char_p, []),
+        "csp_spmv_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+        "csp_adjoint_slots": (C.c_int, [C.c_void_p, P(C.c_size_t)]),
+        "csp_adjoint_pattern": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
         "csp_coo_spmv_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p]),
     }

@@ -599,15 +599,17 @@ int Engine::launches_per_spmv() const
     return n;
 }
 
-int Engine::enqueue_once(cudaStream_t st)
+int Engine::enqueue_parts(const std::vector<Part>& ps, const float* x, float* y, int n, cudaStream_t st)
 {
-    for (const Part& p : parts) {
-        if (bf16) launch_part<__nv_bfloat16>(p, d_x, d_y, width, st);
-        else launch_part<float>(p, d_x, d_y, width, st);
+    for (const Part& p : ps) {
+        if (bf16) launch_part<__nv_bfloat16>(p, x, y, n, st);
+        else launch_part<float>(p, x, y, n, st);
     }
     CSP_CUDA(cudaGetLastError());
     return CSP_OK;
 }
+
+int Engine::enqueue_once(cudaStream_t st) { return enqueue_parts(parts, d_x, d_y, width, st); }
 
 int Engine::spmv(int ntimes)
 {
@@ -672,6 +674,7 @@ int Engine::init(const cocktail_iif* mat, const float* vec, const float* res, in
     if (mat->ifuseell && (rc = add_ell(mat->ell, mat->ell_meth_num))) return rc;
     if (mat->ifusecsr && (rc = add_csr(mat->csr, mat->csr_meth_num))) return rc;
     if (mat->ifusecoo && (rc = add_coo(mat->coo))) return rc;
+    if ((flags & CSP_FLAG_ADJOINT) && (rc = build_adjoint(mat))) return rc;
     CSP_CUDA(cudaDeviceSynchronize());
     return CSP_OK;
 }
@@ -685,9 +688,6 @@ using csp::Engine;
 using csp::set_error;
 using csp::cuda_error;
 
-struct csp_handle {
-    Engine eng;
-};
 
 #define CSP_HANDLE_CHECK(h) \
     do { if (!(h)) return set_error(CSP_EINVAL, "null handle"); } while (0)

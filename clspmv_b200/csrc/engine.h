@@ -34,6 +34,17 @@ struct Part {
     int npad = 0, nwarps = 0;  // COO
 };
 
+enum SegKind { SEG_NONE, SEG_DIA, SEG_LIST, SEG_ELL, SEG_SELL };
+
+// One forward part's share of the value-gradient array (adjoint).
+struct Seg {
+    SegKind kind = SEG_NONE;
+    size_t offset = 0, count = 0;
+    const int* a0 = nullptr;
+    const int* a1 = nullptr;
+    int p0 = 0, p1 = 0, p2 = 0;
+};
+
 struct Engine {
     int width = 0, height = 0, nnz = 0;
     bool bf16 = false;
@@ -48,11 +59,20 @@ struct Engine {
     size_t device_bytes = 0;
     cudaGraphExec_t graph_exec = nullptr;
     cudaStream_t graph_stream = nullptr;
+    // adjoint (CSP_FLAG_ADJOINT)
+    bool adjoint = false;
+    bool abar_blocks = false;          // a block-format part: no value gradients
+    std::vector<Part> adj_parts;       // parts of A^T: xbar += A^T ybar
+    std::vector<Seg> segs;
+    size_t abar_total = 0;
 
     ~Engine();
     int init(const cocktail_iif* mat, const float* vec, const float* res, int flags);
     int spmv(int ntimes);
     int enqueue_once(cudaStream_t st);
+    int enqueue_parts(const std::vector<Part>& ps, const float* x, float* y, int n, cudaStream_t st);
+    int build_adjoint(const cocktail_iif* mat);
+    int launch_abar(const float* ybar, float* abar, int* prow, int* pcol, cudaStream_t st);
     int launches_per_spmv() const;
 
     int alloc(void** p, size_t bytes);
@@ -74,3 +94,8 @@ struct Engine {
 int cuda_error(cudaError_t e, const char* what);
 
 }  // namespace csp
+
+// The opaque handle of the C ABI.
+struct csp_handle {
+    csp::Engine eng;
+};

@@ -1,0 +1,83 @@
+// Value-gradient kernels of the adjoint: abar[slot] = ybar[row(slot)] * x[col(slot)]
+// over every stored slot of a part, in the part's storage order, or -- when `prow`
+// is non-null -- the (row, col) of each slot (row -1 for slots outside the matrix:
+// alignment rows and out-of-range diagonal positions), so a caller can map abar back
+// to matrix entries.  The transposed product itself reuses the forward kernels on
+// transposed parts.
+#pragma once
+
+#include "common.cuh"
+
+namespace csp {
+namespace dev {
+
+__device__ __forceinline__ void put_slot(size_t i, int row, int col, const float* __restrict__ ybar,
+                                         const float* __restrict__ x, float* __restrict__ abar,
+                                         int* __restrict__ prow, int* __restrict__ pcol)
+{
+    if (prow) {
+        prow[i] = row;
+        pcol[i] = row < 0 ? -1 : col;
+    } else {
+        abar[i] = row < 0 ? 0.0f : __ldg(ybar + row) * __ldg(x + col);
+    }
+}
+
+// DIA-layout slots (also BDIA, whose slots carry per-slot offsets): slot (d, r)
+// couples row r with column r + off[d].
+__global__ void __launch_bounds__(256) abar_dia_kernel(const int* __restrict__ off, int nslots_per_row, int len,
+                                                       int m, int n, const float* __restrict__ ybar,
+                                                       const float* __restrict__ x, float* __restrict__ abar,
+                                                       int* __restrict__ prow, int* __restrict__ pcol)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)nslots_per_row * len) return;
+    const int d = (int)(i / len), r = (int)(i % len);
+    const int c = r + __ldg(off + d);
+    const bool in = r < m && c >= 0 && c < n;
+    put_slot(i, in ? r : -1, c, ybar, x, abar, prow, pcol);
+}
+
+// Entry lists with explicit row ids (COO; CSR with its row-id array).
+__global__ void __launch_bounds__(256) abar_list_kernel(const int* __restrict__ rows, const int* __restrict__ cols, int nnz,
+                                                        const float* __restrict__ ybar, const float* __restrict__ x,
+                                                        float* __restrict__ abar, int* __restrict__ prow,
+                                                        int* __restrict__ pcol)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nnz) return;
+    put_slot(i, __ldg(rows + i), __ldg(cols + i), ybar, x, abar, prow, pcol);
+}
+
+// Column-major ELL slots (k, r), r < height_aligned.
+__global__ void __launch_bounds__(256) abar_ell_kernel(const int* __restrict__ col, int ell_num, int hal, int m,
+                                                       const float* __restrict__ ybar, const float* __restrict__ x,
+                                                       float* __restrict__ abar, int* __restrict__ prow,
+                                                       int* __restrict__ pcol)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)ell_num * hal) return;
+    const int r = (int)(i % hal);
+    put_slot(i, r < m ? r : -1, __ldg(col + i), ybar, x, abar, prow, pcol);
+}
+
+// SELL slots: one thread per slice row walks that row's slots.
+__global__ void __launch_bounds__(256) abar_sell_kernel(const int* __restrict__ slice_ptr, const int* __restrict__ col,
+                                                        int H, int nslices, int m, const float* __restrict__ ybar,
+                                                        const float* __restrict__ x, float* __restrict__ abar,
+                                                        int* __restrict__ prow, int* __restrict__ pcol)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nslices * H) return;
+    const int s = t / H, lr = t % H;
+    const int b = __ldg(slice_ptr + s);
+    const int width = (__ldg(slice_ptr + s + 1) - b) / H;
+    const int r = s * H + lr;
+    for (int k = 0; k < width; k++) {
+        const size_t i = (size_t)b + (size_t)k * H + lr;
+        put_slot(i, r < m ? r : -1, __ldg(col + i), ybar, x, abar, prow, pcol);
+    }
+}
+
+}  // namespace dev
+}  // namespace csp

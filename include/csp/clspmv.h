@@ -374,6 +374,26 @@ int csp_spmv_bcsr(coo_matrix_if* coo, int ntimes, csp_report* report);
 int csp_spmv_sbell(coo_matrix_if* coo, int ntimes, csp_report* report);
 
 /* ------------------------------------------------------------------------ */
+/* Adjoint (no counterpart in the reference).  Needs a handle built with      */
+/* CSP_FLAG_ADJOINT, which also stores A^T (a transposed DIA per diagonal      */
+/* part of a square matrix, one transposed CSR for every other part):         */
+/*   d_xbar += A^T * d_ybar            (deterministic, no atomics), and        */
+/*   d_abar[s] = d_ybar[row(s)] * x[col(s)] for every stored slot s of the     */
+/*   forward parts, in launch order, each part in its own storage layout      */
+/*   (DIA/BDIA: diagonal-major slots; CSR/COO: entry order; ELL/SELL: their     */
+/*   slot order) -- the gradient of ybar^T (A x) with respect to the stored    */
+/*   values.  x is the handle's current vector.  All pointers are device       */
+/*   pointers; d_xbar or d_abar may be NULL to skip that output.  Value        */
+/*   gradients of block-format parts are not provided (CSP_EUNSUP).            */
+/* ------------------------------------------------------------------------ */
+int csp_spmv_adjoint(csp_handle* h, const float* d_ybar, float* d_xbar, float* d_abar);
+/* Number of stored slots, the length of d_abar. */
+int csp_adjoint_slots(csp_handle* h, size_t* nslots);
+/* Row and column of every slot (row -1 for slots outside the matrix: alignment
+ * rows, out-of-range diagonal positions), into device arrays of nslots ints. */
+int csp_adjoint_pattern(csp_handle* h, int* d_rows, int* d_cols);
+
+/* ------------------------------------------------------------------------ */
 /* SpMV without device allocation.  No counterpart in the reference.          */
 /*                                                                            */
 /* For callers that cannot allocate device memory -- code running under a     */
