@@ -71,9 +71,22 @@ def make_workload(name: str):
     return desc, (h, w, r, c, v), x, y0
 
 
-def algorithmic_bytes(h, w, nnz, value_bytes=4):
-    """CSR-class minimum per SpMV: values + column ids + row pointers + x once + y read and written."""
+def algorithmic_bytes(h, w, nnz, value_bytes=4, ndiag=None):
+    """Minimum bytes per SpMV, no padding counted: values + indices of the structure class
+    + x once + y read and written.  CSR class: column ids and row pointers; DIA class
+    (ndiag given): one offset per diagonal."""
+    if ndiag is not None:
+        return value_bytes * nnz + 4 * ndiag + 4 * w + 8 * h
     return value_bytes * nnz + 4 * nnz + 4 * (h + 1) + 4 * w + 8 * h
+
+
+def workload_bytes(name, case):
+    """Algorithmic bytes of one SpMV of a workload: banded matrices are counted in the DIA
+    class (their natural storage), the others in the CSR class."""
+    h, w, r, c, v = case
+    if name in ("stencil", "laplacian"):
+        return algorithmic_bytes(h, w, int(r.size), ndiag=int(np.unique(c.astype(np.int64) - r).size))
+    return algorithmic_bytes(h, w, int(r.size))
 
 
 class ClockSampler:
@@ -167,7 +180,7 @@ def cpu_reference_spmv_time(case, x, y0, budget_s: float, min_reps: int = 2):
 
 def run_reference_arm(args, desc, case, x, y0):
     h, w, r, c, v = case
-    ab = algorithmic_bytes(h, w, r.size)
+    ab = workload_bytes(args.workload, case)
     # one step = one whole serial SpMV on one host core; W warm-ups, K timed
     t_step, reps, kind = cpu_reference_spmv_time(case, x, y0, budget_s=0.0, min_reps=args.warmup + args.steps)
     gbs = ab / t_step / 1e9
@@ -216,7 +229,7 @@ def main():
     desc, case, x, y0 = make_workload(args.workload)
     h, w, r, c, v = case
     nnz = int(r.size)
-    ab = algorithmic_bytes(h, w, nnz)
+    ab = workload_bytes(args.workload, case)
     # a dedicated stream: the library and torch (flush, events) must launch on the same one
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -235,27 +248,24 @@ def main():
         torch.cuda.synchronize()
         return [e0.elapsed_time(e1) for e0, e1 in evs]
 
-    # --- on-device autotune over candidate Cocktail partitions (format x kernel) ---
+    # --- the library's on-device autotuner picks the Cocktail partition ---
+    from clspmv_b200 import CSP_ANALYZE_AUTOTUNE, analyze_matrix
     coo = COO(h, w, r, c, v)
-    candidates = [("csr", 2, {}), ("csr", 3, {}), ("csr", 0, {}), ("sell", 0, {"slice_height": 32}), ("coo", 0, {}),
-                  ("csr", 4, {})]
-    tuned = {}
-    for fmt, m, kw in candidates:
-        try:
-            mat = Cocktail.single(fmt, coo, m, **kw)
-            hd = Handle(mat, x, y0)
-        except Exception as e:  # a format that cannot hold the matrix is skipped
-            print(f"# candidate {fmt}/{m} skipped: {e}", file=sys.stderr)
-            continue
-        ms = statistics.median(time_handle(hd, 10, 3))
-        tuned[f"{fmt}{m}"] = (ms, mat, hd)
-    best_key = min(tuned, key=lambda k: tuned[k][0])
-    plain_key = min((k for k in tuned if k in ("csr0", "csr4")), key=lambda k: tuned[k][0])
-    for k, (ms, mat, hd) in tuned.items():
-        if k not in (best_key, plain_key):
-            hd.free()
-    _, best_mat, best = tuned[best_key]
-    plain_ms_med, _, plain_hd = tuned[plain_key]
+    best_mat = analyze_matrix(coo, mode=CSP_ANALYZE_AUTOTUNE)
+    best_key = best_mat.choice
+    best = Handle(best_mat, x, y0)
+    # plain single-format CSR on the same GPU: one warp per row (the reference's vector
+    # kernel design, spmv_all method 2) and one thread per row (method 1); the faster
+    plain = {}
+    for m_ in (0, 4):
+        pm = Cocktail.single("csr", coo, m_)
+        ph = Handle(pm, x, y0)
+        plain[f"csr{m_}"] = (statistics.median(time_handle(ph, 10, 3)), pm, ph)
+    plain_key = min(plain, key=lambda k: plain[k][0])
+    for k_, (_, pm, ph) in plain.items():
+        if k_ != plain_key:
+            ph.free()
+    _, _, plain_hd = plain[plain_key]
 
     # --- timed region: K SpMVs, L2 flushed before each, CUDA events on the launching stream ---
     if world > 1:
@@ -273,9 +283,7 @@ def main():
         total_ms = float(t.item())
         dist.barrier()
     ms_step = total_ms / args.steps
-    value = world * ab / (ms_step * 1e-3) / 1e9
     plain_times = time_handle(plain_hd, max(10, args.steps // 2), 3)
-    plain_gbs = ab / (statistics.median(plain_times) * 1e-3) / 1e9
 
     # --- e2e through the C ABI with pinned host buffers ---
     xp = torch.from_numpy(x).pin_memory()
@@ -311,7 +319,6 @@ def main():
         t = torch.tensor([e2e_ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_ms = float(t.item())
-    e2e_gbs = world * ab / (e2e_ms * 1e-3) / 1e9
 
     peak, peak_kind = _peak()
     kernel_gbs = ab / (statistics.mean(times) * 1e-3) / 1e9
@@ -323,6 +330,9 @@ def main():
         except Exception:
             traffic = None
 
+    value = world * ab / (ms_step * 1e-3) / 1e9
+    e2e_gbs = world * ab / (e2e_ms * 1e-3) / 1e9
+    plain_gbs = ab / (statistics.median(plain_times) * 1e-3) / 1e9
     line = None
     if rank == 0:
         cpu_t, cpu_reps, cpu_kind = cpu_reference_spmv_time(case, x, y0, budget_s=args.cpu_budget)
@@ -331,9 +341,9 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": desc, "nnz": nnz, "algorithmic_bytes_per_spmv": ab,
-                       "partition": best_key, "autotune_ms": {k: t[0] for k, t in tuned.items()},
+                       "partition": best_key,
                        "plain_csr": {"kernel": plain_key, "gb_s": plain_gbs},
-                       "speedup_vs_plain_csr": value / world / plain_gbs,
+                       "speedup_vs_plain_csr": statistics.median(plain_times) / ms_step,
                        "l2": "256 MB write between timed SpMVs (working set < L2)",
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": kernel_gbs, "peak": peak, "unit": "GB/s",
@@ -346,6 +356,7 @@ def main():
         }
     best.free()
     plain_hd.free()
+    best_mat.free()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
