@@ -103,6 +103,11 @@ class csp_analyze_opts(C.Structure):
                 ("flags", C.c_int)]
 
 
+class csp_bandwidth_report(C.Structure):
+    _fields_ = [("launch_us", C.c_double), ("copy_gbs", C.c_double), ("gather_gbs", C.c_double),
+                ("gather_per_s", C.c_double)]
+
+
 class csp_report(C.Structure):
     _fields_ = [("method", C.c_int), ("gflops", C.c_double), ("gbytes", C.c_double), ("ms", C.c_double),
                 ("l2_distance", C.c_double), ("max_diff", C.c_double), ("max_ratio_diff", C.c_double),
@@ -195,6 +200,7 @@ def _declare(lib):
         "csp_spmv_all": (C.c_int, [P(coo_matrix), C.c_int, C.c_int, P(csp_report)]),
         "csp_read_mmf": (C.c_int, [C.c_char_p, P(coo_matrix)]),
         "csp_autotune_choice": (C.c_char_p, []),
+        "csp_bandwidth_test": (C.c_int, [C.c_size_t, C.c_int, P(csp_bandwidth_report)]),
         "csp_spmv_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "csp_adjoint_slots": (C.c_int, [C.c_void_p, P(C.c_size_t)]),
         "csp_adjoint_pattern": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -418,6 +418,19 @@ int csp_coo_spmv_noalloc(int height, int width, int nnz, const int* d_row, const
                          const float* d_x, float* d_y, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* spmv_all method 0 (spmv_all.cpp:196, mem_bandwidth.cpp): device memory      */
+/* bandwidth and kernel launch overhead.  `bytes` per buffer (>= 1 MiB);      */
+/* the gather reads 4-byte values at random indices in [0, gather_range).      */
+/* ------------------------------------------------------------------------ */
+typedef struct csp_bandwidth_report {
+    double launch_us;     /* empty-kernel launch-to-launch time, microseconds      */
+    double copy_gbs;      /* float4 device copy, read + written bytes per second   */
+    double gather_gbs;    /* random gather: index and value bytes per second        */
+    double gather_per_s;  /* random gather: elements per second                      */
+} csp_bandwidth_report;
+int csp_bandwidth_test(size_t bytes, int gather_range, csp_bandwidth_report* rep);
+
+/* ------------------------------------------------------------------------ */
 /* MatrixMarket input (fileio.cpp:10 ReadMMF): 0-based, pattern -> 1.0,       */
 /* symmetric mirrored, sorted.                                               */
 /* ------------------------------------------------------------------------ */
