@@ -120,15 +120,26 @@ def analyze_matrix(coo: COO, mode: int = CSP_ANALYZE_REFERENCE, bench_path: str 
 class Handle:
     """Device engine of one cocktail (cocktail_gpu + cocktail_kernels of the reference)."""
 
-    def __init__(self, mat: Cocktail, vec: np.ndarray | None = None, res: np.ndarray | None = None, flags: int = 0):
-        self._mat = mat
-        self.width, self.height = int(mat.s.mat_width), int(mat.s.mat_height)
+    def __init__(self, mat: Cocktail | None, vec: np.ndarray | None = None, res: np.ndarray | None = None,
+                 flags: int = 0, nrhs: int = 1, bcsr=None):
+        """A handle over `mat` (a Cocktail), or over a generic BCSR struct `bcsr`
+        (csp_init_bcsr_kernels).  With nrhs > 1, vec is width x nrhs and res height x nrhs,
+        row-major."""
+        self._mat = mat if mat is not None else bcsr
+        self.nrhs = int(nrhs)
         v = None if vec is None else np.ascontiguousarray(vec, dtype=np.float32)
         r = None if res is None else np.ascontiguousarray(res, dtype=np.float32)
+        vp = None if v is None else capi.as_ptr(v, C.c_float)
+        rp = None if r is None else capi.as_ptr(r, C.c_float)
         h = C.c_void_p()
-        check(lib().csp_init_mat_kernels(mat.ref(), None if v is None else capi.as_ptr(v, C.c_float),
-                                         None if r is None else capi.as_ptr(r, C.c_float), int(flags), C.byref(h)),
-              "init_mat_kernels")
+        if bcsr is not None:
+            self.width, self.height = int(bcsr.matinfo.width), int(bcsr.matinfo.height)
+            check(lib().csp_init_bcsr_kernels(C.byref(bcsr), vp, rp, self.nrhs, int(flags), C.byref(h)),
+                  "init_bcsr_kernels")
+        else:
+            self.width, self.height = int(mat.s.mat_width), int(mat.s.mat_height)
+            check(lib().csp_init_mat_kernels_ex(mat.ref(), vp, rp, self.nrhs, int(flags), C.byref(h)),
+                  "init_mat_kernels")
         self.h = h
 
     def do_spmv(self, ntimes: int = 1):
@@ -153,7 +164,7 @@ class Handle:
 
     def cpy_result_to_cpu(self, out: np.ndarray | None = None) -> np.ndarray:
         if out is None:
-            out = np.empty(self.height, dtype=np.float32)
+            out = np.empty(self.height * self.nrhs, dtype=np.float32)
         check(lib().csp_cpy_result_to_cpu(self.h, capi.as_ptr(out, C.c_float), out.size), "cpy_result_to_cpu")
         return out
 

@@ -182,6 +182,8 @@ def _declare(lib):
         "csp_analyze_matrix": (C.c_int, [P(coo_matrix), P(cocktail), P(csp_analyze_opts)]),
         "csp_init_mat_kernels": (C.c_int, [P(cocktail), FP, FP, C.c_int, P(C.c_void_p)]),
         "csp_do_spmv": (C.c_int, [C.c_void_p, C.c_int]),
+        "csp_init_mat_kernels_ex": (C.c_int, [P(cocktail), FP, FP, C.c_int, C.c_int, P(C.c_void_p)]),
+        "csp_init_bcsr_kernels": (C.c_int, [P(bcsr_matrix), FP, FP, C.c_int, C.c_int, P(C.c_void_p)]),
         "csp_synchronize": (C.c_int, [C.c_void_p]),
         "csp_cpy_vector_from_cpu": (C.c_int, [C.c_void_p, FP, C.c_int]),
         "csp_cpy_vector_from_gpu": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int]),

@@ -24,6 +24,7 @@
 #include "kernels/flat.cuh"
 #include "kernels/diag.cuh"
 #include "kernels/block.cuh"
+#include "kernels/spmm.cuh"
 
 namespace csp {
 
@@ -475,6 +476,43 @@ int Engine::add_generic_bcsr(const bcsr_matrix_if& b, int method)
 // Launches
 // --------------------------------------------------------------------------
 template <class V>
+static void launch_spmm(const Part& p, const float* x, float* y, int n, int k, cudaStream_t st)
+{
+    using namespace dev;
+    const V* v = static_cast<const V*>(p.v);
+    const int G = k >= 32 ? 32 : (k > 16 ? 32 : (k > 8 ? 16 : (k > 4 ? 8 : (k > 2 ? 4 : 2))));
+    if (p.kind == PART_CSR) {
+        if (p.m == 0) return;
+        const unsigned g = grid_for((long long)p.m * G, kSpmmThreads);
+        switch (G) {
+        case 2: csr_spmm_kernel<V, 2><<<g, kSpmmThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.m, k); break;
+        case 4: csr_spmm_kernel<V, 4><<<g, kSpmmThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.m, k); break;
+        case 8: csr_spmm_kernel<V, 8><<<g, kSpmmThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.m, k); break;
+        case 16: csr_spmm_kernel<V, 16><<<g, kSpmmThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.m, k); break;
+        default: csr_spmm_kernel<V, 32><<<g, kSpmmThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.m, k); break;
+        }
+    } else if (p.kind == PART_GBCSR) {
+        if (p.nbr == 0) return;
+        const unsigned g = grid_for((long long)p.nbr * G, kSpmmThreads);
+#define CSP_GBM(BH, BW)                                                                                                          \
+    do {                                                                                                                         \
+        switch (G) {                                                                                                             \
+        case 2: bcsr_spmm_kernel<V, BH, BW, 2><<<g, kSpmmThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.nbr, p.stride, p.m, n, k); break;   \
+        case 4: bcsr_spmm_kernel<V, BH, BW, 4><<<g, kSpmmThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.nbr, p.stride, p.m, n, k); break;   \
+        case 8: bcsr_spmm_kernel<V, BH, BW, 8><<<g, kSpmmThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.nbr, p.stride, p.m, n, k); break;   \
+        case 16: bcsr_spmm_kernel<V, BH, BW, 16><<<g, kSpmmThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.nbr, p.stride, p.m, n, k); break; \
+        default: bcsr_spmm_kernel<V, BH, BW, 32><<<g, kSpmmThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.nbr, p.stride, p.m, n, k); break; \
+        }                                                                                                                        \
+    } while (0)
+        switch (p.bh * 10 + p.bw) {
+        case 11: CSP_GBM(1, 1); break; case 22: CSP_GBM(2, 2); break; case 33: CSP_GBM(3, 3); break;
+        case 44: CSP_GBM(4, 4); break; case 66: CSP_GBM(6, 6); break;
+        }
+#undef CSP_GBM
+    }
+}
+
+template <class V>
 static void launch_part(const Part& p, const float* x, float* y, int n, cudaStream_t st)
 {
     using namespace dev;
@@ -602,8 +640,13 @@ int Engine::launches_per_spmv() const
 int Engine::enqueue_parts(const std::vector<Part>& ps, const float* x, float* y, int n, cudaStream_t st)
 {
     for (const Part& p : ps) {
-        if (bf16) launch_part<__nv_bfloat16>(p, x, y, n, st);
-        else launch_part<float>(p, x, y, n, st);
+        if (nrhs > 1) {
+            if (bf16) launch_spmm<__nv_bfloat16>(p, x, y, n, nrhs, st);
+            else launch_spmm<float>(p, x, y, n, nrhs, st);
+        } else {
+            if (bf16) launch_part<__nv_bfloat16>(p, x, y, n, st);
+            else launch_part<float>(p, x, y, n, st);
+        }
     }
     CSP_CUDA(cudaGetLastError());
     return CSP_OK;
@@ -639,13 +682,14 @@ int Engine::spmv(int ntimes)
     return CSP_OK;
 }
 
-int Engine::init(const cocktail_iif* mat, const float* vec, const float* res, int flags)
+int Engine::init_common(int w, int h, int nz, const float* vec, const float* res, int flags, int k)
 {
-    if (!mat) return set_error(CSP_EINVAL, "null cocktail");
-    width = mat->mat_width;
-    height = mat->mat_height;
-    nnz = mat->mat_nnz;
+    width = w;
+    height = h;
+    nnz = nz;
     if (width < 0 || height < 0) return set_error(CSP_EINVAL, "negative matrix size");
+    if (k < 1) return set_error(CSP_EINVAL, "nrhs must be >= 1");
+    nrhs = k;
     bf16 = (flags & CSP_FLAG_BF16) != 0;
     use_graph = (flags & CSP_FLAG_GRAPH) != 0;
     int ndev = 0;
@@ -658,12 +702,27 @@ int Engine::init(const cocktail_iif* mat, const float* vec, const float* res, in
     x_len = pad_to(std::max(width, 1), 64) + 64;
     y_len = pad_to(std::max(height, 1), 1024);
     int rc;
-    if ((rc = alloc(reinterpret_cast<void**>(&d_x), (size_t)x_len * 4)) || (rc = alloc(reinterpret_cast<void**>(&d_y), (size_t)y_len * 4)))
+    if ((rc = alloc(reinterpret_cast<void**>(&d_x), (size_t)x_len * nrhs * 4)) ||
+        (rc = alloc(reinterpret_cast<void**>(&d_y), (size_t)y_len * nrhs * 4)))
         return rc;
-    CSP_CUDA(cudaMemset(d_x, 0, (size_t)x_len * 4));
-    CSP_CUDA(cudaMemset(d_y, 0, (size_t)y_len * 4));
-    if (vec && width) CSP_CUDA(cudaMemcpy(d_x, vec, (size_t)width * 4, cudaMemcpyHostToDevice));
-    if (res && height) CSP_CUDA(cudaMemcpy(d_y, res, (size_t)height * 4, cudaMemcpyHostToDevice));
+    CSP_CUDA(cudaMemset(d_x, 0, (size_t)x_len * nrhs * 4));
+    CSP_CUDA(cudaMemset(d_y, 0, (size_t)y_len * nrhs * 4));
+    if (vec && width) CSP_CUDA(cudaMemcpy(d_x, vec, (size_t)width * nrhs * 4, cudaMemcpyHostToDevice));
+    if (res && height) CSP_CUDA(cudaMemcpy(d_y, res, (size_t)height * nrhs * 4, cudaMemcpyHostToDevice));
+    return CSP_OK;
+}
+
+int Engine::init(const cocktail_iif* mat, const float* vec, const float* res, int flags, int k)
+{
+    if (!mat) return set_error(CSP_EINVAL, "null cocktail");
+    int rc = init_common(mat->mat_width, mat->mat_height, mat->mat_nnz, vec, res, flags, k);
+    if (rc) return rc;
+    if (nrhs > 1) {
+        if (mat->ifusebdia || mat->ifusedia || mat->ifusesbell || mat->ifusebell || mat->ifusebcsr || mat->ifusesell ||
+            mat->ifuseell || mat->ifusecoo)
+            return set_error(CSP_EUNSUP, "several right-hand sides run on CSR parts (and csp_init_bcsr_kernels)");
+        if (flags & CSP_FLAG_ADJOINT) return set_error(CSP_EUNSUP, "adjoint with several right-hand sides");
+    }
     // parts, in the reference's launch order
     if (mat->ifusebdia && (rc = add_bdia(mat->bdia, mat->bdia_meth_num))) return rc;
     if (mat->ifusedia && (rc = add_dia(mat->dia, mat->dia_meth_num))) return rc;
@@ -675,6 +734,18 @@ int Engine::init(const cocktail_iif* mat, const float* vec, const float* res, in
     if (mat->ifusecsr && (rc = add_csr(mat->csr, mat->csr_meth_num))) return rc;
     if (mat->ifusecoo && (rc = add_coo(mat->coo))) return rc;
     if ((flags & CSP_FLAG_ADJOINT) && (rc = build_adjoint(mat))) return rc;
+    CSP_CUDA(cudaDeviceSynchronize());
+    return CSP_OK;
+}
+
+int Engine::init_bcsr(const bcsr_matrix_if* b, const float* vec, const float* res, int flags, int k)
+{
+    if (!b) return set_error(CSP_EINVAL, "null BCSR");
+    if (flags & CSP_FLAG_ADJOINT) return set_error(CSP_EUNSUP, "adjoint of a generic BCSR handle");
+    if (k > 1 && b->bcsr_bwidth * b->bcsr_bheight > 36) return set_error(CSP_EUNSUP, "several right-hand sides need blocks of <= 36 elements");
+    int rc = init_common(b->matinfo.width, b->matinfo.height, b->matinfo.nnz, vec, res, flags, k);
+    if (rc) return rc;
+    if ((rc = add_generic_bcsr(*b, 0))) return rc;
     CSP_CUDA(cudaDeviceSynchronize());
     return CSP_OK;
 }
@@ -713,13 +784,30 @@ const char* csp_error_string(int code)
 const char* csp_last_error(void) { return csp::g_last_error.c_str(); }
 const char* csp_version(void) { return "clspmv_b200 0.1.0 (sm_100a)"; }
 
-int csp_init_mat_kernels(const cocktail_iif* mat, const float* vec, const float* res, int flags, csp_handle** out)
+int csp_init_mat_kernels_ex(const cocktail_iif* mat, const float* vec, const float* res, int nrhs, int flags, csp_handle** out)
 {
     if (!out) return set_error(CSP_EINVAL, "null output handle");
     *out = nullptr;
     csp_handle* h = new (std::nothrow) csp_handle();
     if (!h) return set_error(CSP_ENOMEM, "handle");
-    int rc = h->eng.init(mat, vec, res, flags);
+    int rc = h->eng.init(mat, vec, res, flags, nrhs);
+    if (rc) { delete h; return rc; }
+    *out = h;
+    return CSP_OK;
+}
+
+int csp_init_mat_kernels(const cocktail_iif* mat, const float* vec, const float* res, int flags, csp_handle** out)
+{
+    return csp_init_mat_kernels_ex(mat, vec, res, 1, flags, out);
+}
+
+int csp_init_bcsr_kernels(const bcsr_matrix_if* b, const float* vec, const float* res, int nrhs, int flags, csp_handle** out)
+{
+    if (!out) return set_error(CSP_EINVAL, "null output handle");
+    *out = nullptr;
+    csp_handle* h = new (std::nothrow) csp_handle();
+    if (!h) return set_error(CSP_ENOMEM, "handle");
+    int rc = h->eng.init_bcsr(b, vec, res, flags, nrhs);
     if (rc) { delete h; return rc; }
     *out = h;
     return CSP_OK;
@@ -750,27 +838,27 @@ static int copy_in(csp_handle* h, float* dst, int cap, const void* src, int n, c
 int csp_cpy_vector_from_cpu(csp_handle* h, const float* vec, int n)
 {
     CSP_HANDLE_CHECK(h);
-    return copy_in(h, h->eng.d_x, h->eng.width, vec, n, cudaMemcpyHostToDevice);
+    return copy_in(h, h->eng.d_x, h->eng.width * h->eng.nrhs, vec, n, cudaMemcpyHostToDevice);
 }
 int csp_cpy_vector_from_gpu(csp_handle* h, const float* dvec, int n)
 {
     CSP_HANDLE_CHECK(h);
-    return copy_in(h, h->eng.d_x, h->eng.width, dvec, n, cudaMemcpyDeviceToDevice);
+    return copy_in(h, h->eng.d_x, h->eng.width * h->eng.nrhs, dvec, n, cudaMemcpyDeviceToDevice);
 }
 int csp_cpy_result_from_cpu(csp_handle* h, const float* res, int n)
 {
     CSP_HANDLE_CHECK(h);
-    return copy_in(h, h->eng.d_y, h->eng.height, res, n, cudaMemcpyHostToDevice);
+    return copy_in(h, h->eng.d_y, h->eng.height * h->eng.nrhs, res, n, cudaMemcpyHostToDevice);
 }
 int csp_cpy_result_from_gpu(csp_handle* h, const float* dres, int n)
 {
     CSP_HANDLE_CHECK(h);
-    return copy_in(h, h->eng.d_y, h->eng.height, dres, n, cudaMemcpyDeviceToDevice);
+    return copy_in(h, h->eng.d_y, h->eng.height * h->eng.nrhs, dres, n, cudaMemcpyDeviceToDevice);
 }
 int csp_cpy_result_to_cpu(csp_handle* h, float* res, int n)
 {
     CSP_HANDLE_CHECK(h);
-    if (!res || n < 0 || n > h->eng.height) return set_error(CSP_EINVAL, "bad result copy");
+    if (!res || n < 0 || n > h->eng.height * h->eng.nrhs) return set_error(CSP_EINVAL, "bad result copy");
     cudaError_t e = cudaMemcpyAsync(res, h->eng.d_y, (size_t)n * 4, cudaMemcpyDeviceToHost, h->eng.stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->eng.stream);
     return e == cudaSuccess ? CSP_OK : cuda_error(e, "result to cpu");
@@ -778,7 +866,7 @@ int csp_cpy_result_to_cpu(csp_handle* h, float* res, int n)
 int csp_cpy_result_to_gpu(csp_handle* h, float* dres, int n)
 {
     CSP_HANDLE_CHECK(h);
-    if (!dres || n < 0 || n > h->eng.height) return set_error(CSP_EINVAL, "bad result copy");
+    if (!dres || n < 0 || n > h->eng.height * h->eng.nrhs) return set_error(CSP_EINVAL, "bad result copy");
     cudaError_t e = cudaMemcpyAsync(dres, h->eng.d_y, (size_t)n * 4, cudaMemcpyDeviceToDevice, h->eng.stream);
     return e == cudaSuccess ? CSP_OK : cuda_error(e, "result to gpu");
 }

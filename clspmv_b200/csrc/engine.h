@@ -47,6 +47,7 @@ struct Seg {
 
 struct Engine {
     int width = 0, height = 0, nnz = 0;
+    int nrhs = 1;            // right-hand sides: x is width x nrhs, y height x nrhs, row-major
     bool bf16 = false;
     bool use_graph = false;
     cudaStream_t own_stream = nullptr;
@@ -67,7 +68,9 @@ struct Engine {
     size_t abar_total = 0;
 
     ~Engine();
-    int init(const cocktail_iif* mat, const float* vec, const float* res, int flags);
+    int init(const cocktail_iif* mat, const float* vec, const float* res, int flags, int k = 1);
+    int init_common(int w, int h, int nz, const float* vec, const float* res, int flags, int k);
+    int init_bcsr(const bcsr_matrix_if* b, const float* vec, const float* res, int flags, int k);
     int spmv(int ntimes);
     int enqueue_once(cudaStream_t st);
     int enqueue_parts(const std::vector<Part>& ps, const float* x, float* y, int n, cudaStream_t st);

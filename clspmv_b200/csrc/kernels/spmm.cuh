@@ -1,0 +1,105 @@
+// Multiple right-hand sides: Y += A * X with X (n x k) and Y (m x k) row-major, so
+// the k values of one column index are contiguous and every gather is a coalesced
+// row segment.  A lane group of G = min(k, 32) lanes serves one (block) row, lane l
+// owning right-hand sides l, l + G, ...; the group's entries are staged in shared
+// memory by coalesced loads and read back as broadcasts.
+#pragma once
+
+#include "common.cuh"
+
+namespace csp {
+namespace dev {
+
+constexpr int kSpmmThreads = 256;
+
+// CSR: one group per row.
+template <class V, int G>
+__global__ void __launch_bounds__(kSpmmThreads) csr_spmm_kernel(const int* __restrict__ rp, const int* __restrict__ col,
+                                                                const V* __restrict__ val, const float* __restrict__ x,
+                                                                float* __restrict__ y, int m, int k)
+{
+    __shared__ int s_col[kSpmmThreads];
+    __shared__ float s_val[kSpmmThreads];
+    const int lane = threadIdx.x % G;
+    const int gbase = threadIdx.x - lane;   // this group's slice of the staging arrays
+    // groups of one warp run different trip counts: each synchronises only its own lanes
+    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) - lane));
+    const int row = (int)(((long long)blockIdx.x * kSpmmThreads + threadIdx.x) / G);
+    const bool valid = row < m;
+    const int s = valid ? __ldg(rp + row) : 0, e = valid ? __ldg(rp + row + 1) : 0;
+    for (int c0 = 0; c0 < k; c0 += G) {
+        const int c = c0 + lane;
+        float acc = 0.0f;
+        for (int j0 = s; j0 < e; j0 += G) {
+            const int n = min(G, e - j0);
+            __syncwarp(gmask);
+            if (lane < n) {
+                s_col[gbase + lane] = __ldg(col + j0 + lane);
+                s_val[gbase + lane] = Val<V>::ld(val + j0 + lane);
+            }
+            __syncwarp(gmask);
+            if (c < k)
+                for (int t = 0; t < n; t++) acc += s_val[gbase + t] * __ldg(x + (size_t)s_col[gbase + t] * k + c);
+        }
+        if (valid && c < k) y[(size_t)row * k + c] += acc;
+    }
+}
+
+// Generic BCSR (block-element-major data[e * aligned + block]): one group per block row.
+// The staged block values take kSpmmThreads * BH * BW floats of shared memory, so
+// blocks are limited to 36 elements (6 x 6).
+template <class V, int BH, int BW, int G>
+__global__ void __launch_bounds__(kSpmmThreads) bcsr_spmm_kernel(const int* __restrict__ rp, const int* __restrict__ col,
+                                                                 const V* __restrict__ data, const float* __restrict__ x,
+                                                                 float* __restrict__ y, int nbr, int aligned, int m, int n,
+                                                                 int k)
+{
+    constexpr int BS = BH * BW;
+    __shared__ float s_val[kSpmmThreads * BS];
+    __shared__ int s_col[kSpmmThreads];
+    const int lane = threadIdx.x % G;
+    const int gbase = threadIdx.x - lane;
+    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) - lane));
+    const int br = (int)(((long long)blockIdx.x * kSpmmThreads + threadIdx.x) / G);
+    const bool valid = br < nbr;
+    const int s = valid ? __ldg(rp + br) : 0, e = valid ? __ldg(rp + br + 1) : 0;
+    for (int c0 = 0; c0 < k; c0 += G) {
+        const int c = c0 + lane;
+        float acc[BH];
+#pragma unroll
+        for (int h = 0; h < BH; h++) acc[h] = 0.0f;
+        for (int j0 = s; j0 < e; j0 += G) {
+            const int nb = min(G, e - j0);
+            __syncwarp(gmask);
+            if (lane < nb) {
+                s_col[gbase + lane] = __ldg(col + j0 + lane);
+#pragma unroll
+                for (int q = 0; q < BS; q++) s_val[(gbase + lane) * BS + q] = Val<V>::ld(data + (size_t)q * aligned + j0 + lane);
+            }
+            __syncwarp(gmask);
+            if (c < k) {
+                for (int t = 0; t < nb; t++) {
+                    const int bc = s_col[gbase + t];
+                    const float* bv = s_val + (gbase + t) * BS;
+                    float xv[BW];
+#pragma unroll
+                    for (int w = 0; w < BW; w++) xv[w] = (bc + w < n) ? __ldg(x + (size_t)(bc + w) * k + c) : 0.0f;
+#pragma unroll
+                    for (int h = 0; h < BH; h++)
+#pragma unroll
+                        for (int w = 0; w < BW; w++) acc[h] += bv[h * BW + w] * xv[w];
+                }
+            }
+        }
+        if (valid && c < k) {
+#pragma unroll
+            for (int h = 0; h < BH; h++) {
+                const int r = br * BH + h;
+                if (r < m) y[(size_t)r * k + c] += acc[h];
+            }
+        }
+    }
+}
+
+}  // namespace dev
+}  // namespace csp

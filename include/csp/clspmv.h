@@ -315,6 +315,17 @@ typedef struct csp_handle csp_handle;
  * res (length mat_height; may be NULL for zeros), and select one kernel per
  * sub-matrix from its *_meth_num.  (spmv_cocktail.cpp:1593 init_mat_kernels) */
 int csp_init_mat_kernels(const cocktail_iif* mat, const float* vec, const float* res, int flags, csp_handle** out);
+/* Several right-hand sides (SpMM, no counterpart in the reference):
+ * res (mat_height x nrhs) += A * vec (mat_width x nrhs), both row-major, so the
+ * copy functions take nrhs times as many floats.  nrhs > 1 runs on CSR parts only;
+ * other formats return CSP_EUNSUP (use csp_init_bcsr_kernels for block matrices). */
+int csp_init_mat_kernels_ex(const cocktail_iif* mat, const float* vec, const float* res, int nrhs, int flags,
+                            csp_handle** out);
+/* A handle over one generic BCSR matrix (matrix_storage.h:169 layout, any block
+ * shape 1x1, 2x2, 3x3, 4x4, 6x6 or 8x8; nrhs > 1 up to 6x6), e.g. the 3x3-block FEM
+ * case the b4 formats cannot hold.  Same do_spmv / copy calls. */
+int csp_init_bcsr_kernels(const bcsr_matrix_if* mat, const float* vec, const float* res, int nrhs, int flags,
+                          csp_handle** out);
 /* Enqueue ntimes SpMVs res += A*vec on the handle's stream.  (:1091 do_spmv) */
 int csp_do_spmv(csp_handle* h, int ntimes);
 /* Block until every launch on the handle's stream has finished. */
