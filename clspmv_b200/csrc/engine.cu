@@ -491,6 +491,25 @@ static void launch_spmm(const Part& p, const float* x, float* y, int n, int k, c
         case 16: csr_spmm_kernel<V, 16><<<g, kSpmmThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.m, k); break;
         default: csr_spmm_kernel<V, 32><<<g, kSpmmThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.m, k); break;
         }
+    } else if (p.kind == PART_GBCSR && k % 4 == 0) {
+        // register-blocked: CW lanes x 4 right-hand sides, 4 sub-groups over the blocks
+        if (p.nbr == 0) return;
+        const int CW = k >= 32 ? 8 : (k >= 16 ? 4 : (k >= 8 ? 2 : 1));
+        const unsigned g = grid_for((long long)p.nbr * CW * 4, kSpmmThreads);
+#define CSP_GB4(BH, BW)                                                                                                          \
+    do {                                                                                                                         \
+        switch (CW) {                                                                                                            \
+        case 1: bcsr_spmm4_kernel<V, BH, BW, 1, 4><<<g, kSpmmThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.nbr, p.stride, p.m, n, k); break; \
+        case 2: bcsr_spmm4_kernel<V, BH, BW, 2, 4><<<g, kSpmmThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.nbr, p.stride, p.m, n, k); break; \
+        case 4: bcsr_spmm4_kernel<V, BH, BW, 4, 4><<<g, kSpmmThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.nbr, p.stride, p.m, n, k); break; \
+        default: bcsr_spmm4_kernel<V, BH, BW, 8, 4><<<g, kSpmmThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.nbr, p.stride, p.m, n, k); break; \
+        }                                                                                                                        \
+    } while (0)
+        switch (p.bh * 10 + p.bw) {
+        case 11: CSP_GB4(1, 1); break; case 22: CSP_GB4(2, 2); break; case 33: CSP_GB4(3, 3); break;
+        case 44: CSP_GB4(4, 4); break; case 66: CSP_GB4(6, 6); break;
+        }
+#undef CSP_GB4
     } else if (p.kind == PART_GBCSR) {
         if (p.nbr == 0) return;
         const unsigned g = grid_for((long long)p.nbr * G, kSpmmThreads);

@@ -101,5 +101,94 @@ __global__ void __launch_bounds__(kSpmmThreads) bcsr_spmm_kernel(const int* __re
     }
 }
 
+// Generic BCSR with k a multiple of 4: register-blocked.  A block row is served by
+// L = CW * S lanes: CW lanes each own 4 consecutive right-hand sides (128-bit loads of
+// X and Y rows) and S sub-groups split the block row's blocks, summed by shuffles at
+// the end.  Block values are staged element-major -> shared memory by coalesced loads
+// (one block per lane of the group) and read back as broadcasts.  Columns beyond
+// 4 * CW are handled in further passes.
+template <class V, int BH, int BW, int CW, int S>
+__global__ void __launch_bounds__(kSpmmThreads) bcsr_spmm4_kernel(const int* __restrict__ rp, const int* __restrict__ col,
+                                                                  const V* __restrict__ data, const float* __restrict__ x,
+                                                                  float* __restrict__ y, int nbr, int aligned, int m, int n,
+                                                                  int k)
+{
+    constexpr int BS = BH * BW;
+    constexpr int L = CW * S;
+    __shared__ float s_val[kSpmmThreads * BS];
+    __shared__ int s_col[kSpmmThreads];
+    const int lane = threadIdx.x % L;
+    const int cw = lane % CW, sub = lane / CW;
+    const int gbase = threadIdx.x - lane;
+    const unsigned gmask = (L == 32) ? 0xffffffffu : (((1u << L) - 1u) << ((threadIdx.x & 31) - lane));
+    const int br = (int)(((long long)blockIdx.x * kSpmmThreads + threadIdx.x) / L);
+    const bool valid = br < nbr;
+    const int s = valid ? __ldg(rp + br) : 0, e = valid ? __ldg(rp + br + 1) : 0;
+    for (int c0 = 0; c0 < k; c0 += 4 * CW) {
+        const int c = c0 + 4 * cw;
+        const bool active = c < k;
+        float4 acc[BH];
+#pragma unroll
+        for (int h = 0; h < BH; h++) acc[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int j0 = s; j0 < e; j0 += L) {
+            const int nb = min(L, e - j0);
+            __syncwarp(gmask);
+            if (lane < nb) {
+                s_col[gbase + lane] = __ldg(col + j0 + lane);
+#pragma unroll
+                for (int q = 0; q < BS; q++) s_val[(gbase + lane) * BS + q] = Val<V>::ld(data + (size_t)q * aligned + j0 + lane);
+            }
+            __syncwarp(gmask);
+            if (active) {
+                for (int t = sub; t < nb; t += S) {
+                    const int bc = s_col[gbase + t];
+                    const float* bv = s_val + (gbase + t) * BS;
+                    float4 xv[BW];
+#pragma unroll
+                    for (int w = 0; w < BW; w++)
+                        xv[w] = (bc + w < n) ? __ldg(reinterpret_cast<const float4*>(x + (size_t)(bc + w) * k + c))
+                                             : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+                    for (int h = 0; h < BH; h++)
+#pragma unroll
+                        for (int w = 0; w < BW; w++) {
+                            const float a = bv[h * BW + w];
+                            acc[h].x += a * xv[w].x;
+                            acc[h].y += a * xv[w].y;
+                            acc[h].z += a * xv[w].z;
+                            acc[h].w += a * xv[w].w;
+                        }
+                }
+            }
+        }
+        // sum the S sub-groups (lanes cw, cw + CW, ...)
+#pragma unroll
+        for (int h = 0; h < BH; h++) {
+#pragma unroll
+            for (int o = CW; o < L; o <<= 1) {
+                acc[h].x += __shfl_xor_sync(gmask, acc[h].x, o, L);
+                acc[h].y += __shfl_xor_sync(gmask, acc[h].y, o, L);
+                acc[h].z += __shfl_xor_sync(gmask, acc[h].z, o, L);
+                acc[h].w += __shfl_xor_sync(gmask, acc[h].w, o, L);
+            }
+        }
+        if (valid && active && sub == 0) {
+#pragma unroll
+            for (int h = 0; h < BH; h++) {
+                const int r = br * BH + h;
+                if (r < m) {
+                    float4* yp = reinterpret_cast<float4*>(y + (size_t)r * k + c);
+                    float4 o = *yp;
+                    o.x += acc[h].x;
+                    o.y += acc[h].y;
+                    o.z += acc[h].z;
+                    o.w += acc[h].w;
+                    *yp = o;
+                }
+            }
+        }
+    }
+}
+
 }  // namespace dev
 }  // namespace csp
