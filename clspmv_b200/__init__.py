@@ -27,7 +27,9 @@ from .capi import (COO, CSP_ANALYZE_AUTOTUNE, CSP_ANALYZE_REFERENCE, CSP_FLAG_AD
 
 __all__ = ["COO", "Cocktail", "Handle", "analyze_matrix", "init_mat_kernels", "spmv_all", "evaluate",
            "CspError", "CSP_FLAG_BF16", "CSP_FLAG_GRAPH", "CSP_FLAG_USE_TEX", "CSP_FLAG_ADJOINT",
-           "CSP_ANALYZE_REFERENCE", "CSP_ANALYZE_AUTOTUNE", "lib"]
+           "CSP_ANALYZE_REFERENCE", "CSP_ANALYZE_AUTOTUNE", "lib", "Batch"]
+
+from .batch import Batch  # noqa: E402
 
 FORMATS = ("bdia", "dia", "sbell", "bell", "bcsr", "sell", "ell", "csr", "coo")
 

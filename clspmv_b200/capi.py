@@ -22,6 +22,13 @@ CSP_OK, CSP_EINVAL, CSP_ENOMEM, CSP_ECUDA, CSP_EFORMAT, CSP_ENODEV, CSP_EUNSUP, 
 CSP_FLAG_USE_TEX, CSP_FLAG_BF16, CSP_FLAG_GRAPH, CSP_FLAG_ADJOINT = 0x1, 0x2, 0x4, 0x8
 CSP_ANALYZE_REFERENCE, CSP_ANALYZE_AUTOTUNE = 0, 1
 CSP_NOALLOC_MAX_NNZ = 33554432
+CSP_BFMT_AUTO = -1
+(CSP_BFMT_CSR, CSP_BFMT_SELL32, CSP_BFMT_SELL128, CSP_BFMT_DIA, CSP_BFMT_BCSR2, CSP_BFMT_BCSR3,
+ CSP_BFMT_BCSR4, CSP_BFMT_COUNT) = range(8)
+BFMT_NAMES = ("csr", "sell32", "sell128", "dia", "bcsr2", "bcsr3", "bcsr4")
+CSP_BATCH_TUNE_MODEL, CSP_BATCH_TUNE_DEVICE = 0, 1
+CSP_BATCH_FWD, CSP_BATCH_ADJ = 1, 2
+CSP_BV_X, CSP_BV_Y, CSP_BV_YBAR, CSP_BV_XBAR, CSP_BV_ABAR = range(5)
 
 
 class matrixInfo(C.Structure):
@@ -101,6 +108,16 @@ class cocktail(C.Structure):
 class csp_analyze_opts(C.Structure):
     _fields_ = [("mode", C.c_int), ("bench_path", C.c_char_p), ("verbose", C.c_int), ("cache_path", C.c_char_p),
                 ("flags", C.c_int)]
+
+
+class csp_batch_opts(C.Structure):
+    _fields_ = [("flags", C.c_int), ("format", C.c_int), ("tune", C.c_int), ("cache_path", C.c_char_p)]
+
+
+class csp_batch_features(C.Structure):
+    _fields_ = [("rows", C.c_int), ("cols", C.c_int), ("nnz", C.c_int), ("max_row", C.c_int), ("ndiag", C.c_int),
+                ("dia_slots", C.c_longlong), ("sell_slots", C.c_longlong * 2), ("bcsr_blocks", C.c_longlong * 3),
+                ("feasible", C.c_uint), ("model_format", C.c_int), ("signature", C.c_ulonglong)]
 
 
 class csp_bandwidth_report(C.Structure):
@@ -208,6 +225,22 @@ def _declare(lib):
         "csp_adjoint_pattern": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),
         "csp_coo_spmv_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p]),
+        "csp_batch_features_of": (C.c_int, [P(coo_matrix), C.c_int, P(csp_batch_features)]),
+        "csp_batch_create": (C.c_int, [P(P(coo_matrix)), C.c_int, P(csp_batch_opts), P(C.c_void_p)]),
+        "csp_batch_free": (C.c_int, [C.c_void_p]),
+        "csp_batch_layout": (C.c_int, [C.c_void_p, P(C.c_longlong), P(C.c_longlong), P(C.c_longlong)]),
+        "csp_batch_formats": (C.c_int, [C.c_void_p, IP]),
+        "csp_batch_device_ptrs": (C.c_int, [C.c_void_p, P(C.c_void_p), P(C.c_void_p), P(C.c_void_p), P(C.c_void_p),
+                                            P(C.c_void_p)]),
+        "csp_batch_copy": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+        "csp_batch_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+        "csp_batch_get_stream": (C.c_void_p, [C.c_void_p]),
+        "csp_batch_run": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+        "csp_batch_run_plain": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int]),
+        "csp_batch_synchronize": (C.c_int, [C.c_void_p]),
+        "csp_batch_launches": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+        "csp_batch_device_bytes": (C.c_size_t, [C.c_void_p]),
+        "csp_batch_pattern": (C.c_int, [C.c_void_p, C.c_int, IP, IP]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -82,16 +82,6 @@ int Engine::upload_int(int** d, const int* h, size_t n, size_t cap)
     return CSP_OK;
 }
 
-// Round-to-nearest-even FP32 -> BF16 (NaN kept quiet).
-static inline uint16_t to_bf16(float f)
-{
-    uint32_t u;
-    memcpy(&u, &f, 4);
-    if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40);
-    u += 0x7fffu + ((u >> 16) & 1u);
-    return (uint16_t)(u >> 16);
-}
-
 // Matrix values in the handle's storage type (FP32, or BF16 with CSP_FLAG_BF16).
 int Engine::upload_val(void** d, const float* h, size_t n, size_t cap)
 {
@@ -138,6 +128,41 @@ static int check_row_ptr(const int* rp, int rows, const char* what)
 }
 static inline unsigned grid_for(long long threads, int block) { return (unsigned)((threads + block - 1) / block); }
 
+// CSR adaptive work blocks: chunks of rows longer than kAdaptNnz first, then runs of
+// whole rows (at most kAdaptThreads rows, at most kAdaptNnz entries each).
+void make_adaptive_blocks(const int* rp, int m, std::vector<int4>& blocks, std::vector<int4>& longs, int& nslots)
+{
+    std::vector<int4> runs;
+    blocks.clear();
+    longs.clear();
+    nslots = 0;
+    int r = 0;
+    while (r < m) {
+        const int len = rp[r + 1] - rp[r];
+        if (len > dev::kAdaptNnz) {
+            const int lid = (int)longs.size();
+            const int nch = (len + dev::kAdaptNnz - 1) / dev::kAdaptNnz;
+            longs.push_back(make_int4(r, nslots, nch, 0));
+            for (int k = 0; k < nch; k++)
+                blocks.push_back(make_int4(k, -(lid + 1), rp[r] + k * dev::kAdaptNnz,
+                                           std::min(rp[r] + (k + 1) * dev::kAdaptNnz, rp[r + 1])));
+            nslots += nch;
+            r++;
+            continue;
+        }
+        const int start = r;
+        long long acc = 0;
+        while (r < m && r - start < dev::kAdaptThreads) {
+            const int l = rp[r + 1] - rp[r];
+            if (l > dev::kAdaptNnz || acc + l > dev::kAdaptNnz) break;
+            acc += l;
+            r++;
+        }
+        runs.push_back(make_int4(start, r - start, rp[start], rp[r]));
+    }
+    blocks.insert(blocks.end(), runs.begin(), runs.end());
+}
+
 // --------------------------------------------------------------------------
 // Per-format setup.  Each validates the struct, uploads it and fixes the launch.
 // --------------------------------------------------------------------------
@@ -177,36 +202,9 @@ int Engine::add_csr(const csr_matrix_if& c, int method)
             return rc;
     }
     if (method == 2) {
-        // work blocks: chunks of long rows first, then runs of whole rows
-        std::vector<int4> chunks, runs, longs;
+        std::vector<int4> blocks, longs;
         int nslots = 0;
-        int r = 0;
-        const int* rp = c.csr_row_ptr;
-        while (r < m) {
-            const int len = rp[r + 1] - rp[r];
-            if (len > dev::kAdaptNnz) {
-                const int lid = (int)longs.size();
-                const int nch = (len + dev::kAdaptNnz - 1) / dev::kAdaptNnz;
-                longs.push_back(make_int4(r, nslots, nch, 0));
-                for (int k = 0; k < nch; k++)
-                    chunks.push_back(make_int4(k, -(lid + 1), rp[r] + k * dev::kAdaptNnz,
-                                               std::min(rp[r] + (k + 1) * dev::kAdaptNnz, rp[r + 1])));
-                nslots += nch;
-                r++;
-                continue;
-            }
-            const int start = r;
-            long long acc = 0;
-            while (r < m && r - start < dev::kAdaptThreads) {
-                const int l = rp[r + 1] - rp[r];
-                if (l > dev::kAdaptNnz || acc + l > dev::kAdaptNnz) break;
-                acc += l;
-                r++;
-            }
-            runs.push_back(make_int4(start, r - start, rp[start], rp[r]));
-        }
-        std::vector<int4> blocks(chunks);
-        blocks.insert(blocks.end(), runs.begin(), runs.end());
+        make_adaptive_blocks(c.csr_row_ptr, m, blocks, longs, nslots);
         p.nblocks = (int)blocks.size();
         if ((rc = alloc(reinterpret_cast<void**>(&p.blocks), std::max<size_t>(blocks.size(), 1) * sizeof(int4))) ||
             (rc = alloc(reinterpret_cast<void**>(&p.long_rows), std::max<size_t>(longs.size(), 1) * sizeof(int4))) ||
@@ -255,9 +253,24 @@ int Engine::add_coo(const coo_matrix_if& c)
     if ((rc = upload_int(&p.i0, r.data(), npad, npad)) || (rc = upload_int(&p.i1, cl.data(), npad, npad)) ||
         (rc = upload_val(&p.v, v.data(), npad, npad)))
         return rc;
-    if ((rc = alloc(reinterpret_cast<void**>(&p.scratch_row), (size_t)2 * p.nwarps * sizeof(int))) ||
+    // rows that cross a chunk boundary ("spans", see coo_segment_kernel)
+    std::vector<int> span_head((size_t)p.nwarps, -1);
+    std::vector<int4> spans;
+    for (int w = 1; w < p.nwarps; w++) {
+        const int b = w * dev::kCooChunk;
+        if (r[b - 1] != r[b]) continue;
+        if (!spans.empty() && spans.back().x == r[b] && spans.back().y + spans.back().z == w) spans.back().z++;
+        else spans.push_back(make_int4(r[b], w - 1, 2, 0));
+        span_head[w] = (int)spans.size() - 1;
+    }
+    const size_t ns = std::max<size_t>(spans.size(), 1);
+    if ((rc = upload_int(&p.span_head, span_head.data(), span_head.size(), span_head.size())) ||
+        (rc = alloc(reinterpret_cast<void**>(&p.spans), ns * sizeof(int4))) ||
+        (rc = alloc(reinterpret_cast<void**>(&p.scratch_row), ns * sizeof(int))) ||
         (rc = alloc(reinterpret_cast<void**>(&p.scratch_val), (size_t)2 * p.nwarps * sizeof(float))))
         return rc;
+    if (!spans.empty()) CSP_CUDA(cudaMemcpy(p.spans, spans.data(), spans.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    CSP_CUDA(cudaMemset(p.scratch_row, 0, ns * sizeof(int)));   // arrival counters
     parts.push_back(p);
     return CSP_OK;
 }
@@ -563,8 +576,8 @@ static void launch_part(const Part& p, const float* x, float* y, int n, cudaStre
     }
     case PART_COO: {
         coo_segment_kernel<V><<<grid_for((long long)p.nwarps * 32, 256), 256, 0, st>>>(p.i0, p.i1, v, x, y, p.npad, p.nwarps,
-                                                                                      p.scratch_row, p.scratch_val);
-        coo_fixup_kernel<<<grid_for(2LL * p.nwarps, 256), 256, 0, st>>>(p.scratch_row, p.scratch_val, 2 * p.nwarps, y);
+                                                                                      p.span_head, p.spans, p.scratch_row,
+                                                                                      p.scratch_val);
         break;
     }
     case PART_ELL:
@@ -651,9 +664,7 @@ static void launch_part(const Part& p, const float* x, float* y, int n, cudaStre
 
 int Engine::launches_per_spmv() const
 {
-    int n = 0;
-    for (const Part& p : parts) n += (p.kind == PART_COO) ? 2 : 1;
-    return n;
+    return (int)parts.size();
 }
 
 int Engine::enqueue_parts(const std::vector<Part>& ps, const float* x, float* y, int n, cudaStream_t st)

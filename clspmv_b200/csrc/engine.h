@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 #include <stddef.h>
+#include <stdint.h>
+#include <string.h>
 #include <vector>
 
 #include "csp/clspmv.h"
@@ -20,8 +22,10 @@ struct Part {
     int4* blocks = nullptr;     // CSR adaptive work blocks
     int4* long_rows = nullptr;  // CSR adaptive long rows {row, first slot, chunks, -}
     void* v = nullptr;   // values (FP32 or BF16)
-    int* scratch_row = nullptr;   // COO chunk heads/tails; CSR adaptive arrival counters
-    float* scratch_val = nullptr; // COO partial sums; CSR adaptive long-row partials
+    int* scratch_row = nullptr;   // COO span / CSR adaptive long-row arrival counters
+    float* scratch_val = nullptr; // COO chunk shares of spans; CSR adaptive long-row partials
+    int* span_head = nullptr;     // COO: span continued by each chunk's first row, or -1
+    int4* spans = nullptr;        // COO: rows crossing chunk boundaries {row, first chunk, chunks, -}
     int m = 0;        // rows (or block rows' parent height)
     int nnz = 0;
     int k = 0;        // ELL width / #diagonals / #bands / BELL slots
@@ -95,6 +99,20 @@ struct Engine {
 };
 
 int cuda_error(cudaError_t e, const char* what);
+
+// CSR adaptive work blocks (see csr_adaptive_kernel) of rows [0, m) of row pointer rp;
+// nslots = long-row chunk partial slots.
+void make_adaptive_blocks(const int* rp, int m, std::vector<int4>& blocks, std::vector<int4>& longs, int& nslots);
+
+// Round-to-nearest-even FP32 -> BF16 (NaN kept quiet).
+inline uint16_t to_bf16(float f)
+{
+    uint32_t u;
+    memcpy(&u, &f, 4);
+    if ((u & 0x7fffffffu) > 0x7f800000u) return (uint16_t)((u >> 16) | 0x40);
+    u += 0x7fffu + ((u >> 16) & 1u);
+    return (uint16_t)(u >> 16);
+}
 
 }  // namespace csp
 

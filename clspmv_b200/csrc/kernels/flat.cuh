@@ -244,13 +244,16 @@ __global__ void __launch_bounds__(kAdaptThreads) csr_adaptive_kernel(const int* 
 // Each warp owns a chunk of kCooTiles tiles of 128 entries (4 per lane, 128-bit
 // loads).  Inside a tile, lanes reduce their 4 entries, a keyed shuffle scan over
 // lanes joins row segments that cross lanes, and a running carry joins segments
-// that cross tiles.  Rows that begin and end inside the chunk are added to y by
-// the one lane that closes them.  The chunk's first row segment ("head") and its
-// still-open last segment ("tail") go to a scratch array of (row, partial) pairs;
-// coo_fixup_kernel then adds every run of equal rows there in order.  No atomics:
-// every y entry has a single writer per kernel and the result is deterministic.
-// Requires the arrays padded to a multiple of 128 entries with (last row, last
-// col, 0.0) and rows sorted.
+// that cross tiles.  Rows that lie inside one chunk are added to y by the one lane
+// that closes them.  A row that crosses a chunk boundary is a "span", found by the
+// host when the matrix is uploaded: spans[s] = {row, first chunk, chunks, -} and
+// span_of_head[w] = the span that chunk w's first row continues, or -1.  Each chunk
+// writes its share of a span to part_val (slot 2w for the chunk's first row, 2w + 1
+// for its last) and counts itself on the span's arrival counter; the chunk that
+// arrives last adds the shares in chunk order to y and resets the counter.  No
+// atomics on y and no second pass: every y entry has a single writer per launch and
+// the result is deterministic.  Requires the arrays padded to a multiple of 128
+// entries with (last row, last col, 0.0) and rows sorted.
 // ---------------------------------------------------------------------------
 constexpr int kCooTiles = 4;
 constexpr int kCooChunk = 128 * kCooTiles;
@@ -259,7 +262,8 @@ template <class V>
 __global__ void __launch_bounds__(256) coo_segment_kernel(const int* __restrict__ rowid, const int* __restrict__ colid,
                                                           const V* __restrict__ val, const float* __restrict__ x,
                                                           float* __restrict__ y, int nnz_pad, int nwarps,
-                                                          int* __restrict__ part_row, float* __restrict__ part_val)
+                                                          const int* __restrict__ span_of_head, const int4* __restrict__ spans,
+                                                          int* __restrict__ span_count, float* __restrict__ part_val)
 {
     const int lane = threadIdx.x & 31;
     const int w = (int)(((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -267,7 +271,10 @@ __global__ void __launch_bounds__(256) coo_segment_kernel(const int* __restrict_
     const int base = w * kCooChunk;
     const int end = min(base + kCooChunk, nnz_pad);
     const int head_row = __ldg(rowid + base);
-    bool head_open = true;
+    const int head_span = __ldg(span_of_head + w);
+    const int next_span = (w + 1 < nwarps) ? __ldg(span_of_head + w + 1) : -1;
+    // the head segment stays open (deferred to part_val) only if the row began earlier
+    bool head_open = head_span >= 0;
     int carry_row = head_row;
     float carry_val = 0.0f;
 
@@ -298,7 +305,6 @@ __global__ void __launch_bounds__(256) coo_segment_kernel(const int* __restrict_
         if (tile_first != carry_row) {
             if (lane == 0) {
                 if (head_open && carry_row == head_row) {
-                    part_row[2 * w] = carry_row;
                     part_val[2 * w] = carry_val;
                 } else {
                     y[carry_row] += carry_val;
@@ -338,7 +344,6 @@ __global__ void __launch_bounds__(256) coo_segment_kernel(const int* __restrict_
             const bool closes = !last_in_lane ? (nxt != rr[k]) : (lane < 31 && nxt != rr[k]);
             if (closes) {
                 if (head_open && rr[k] == head_row) {
-                    part_row[2 * w] = rr[k];
                     part_val[2 * w] = run;
                     closed_head = true;
                 } else {
@@ -352,30 +357,40 @@ __global__ void __launch_bounds__(256) coo_segment_kernel(const int* __restrict_
         carry_val = __shfl_sync(0xffffffffu, run, 31);
         if (__any_sync(0xffffffffu, closed_head)) head_open = false;
     }
-    if (lane == 0) {
-        if (head_open) {
-            part_row[2 * w] = carry_row;      // == head_row: the chunk is one open segment
-            part_val[2 * w] = carry_val;
-            part_row[2 * w + 1] = carry_row;
-            part_val[2 * w + 1] = 0.0f;
-        } else {
-            part_row[2 * w + 1] = carry_row;
-            part_val[2 * w + 1] = carry_val;
+    // the segment still open at the end of the chunk: its row continues into the next
+    // chunk exactly when that chunk's head belongs to a span
+    int arrive0 = -1, arrive1 = -1;
+    if (head_open) {
+        // the whole chunk lies in the head row, which began in an earlier chunk
+        if (lane == 0) part_val[2 * w] = carry_val;
+        arrive0 = head_span;
+    } else {
+        if (head_span >= 0) arrive0 = head_span;   // its share was written when the head closed
+        if (next_span >= 0) {
+            if (lane == 0) part_val[2 * w + 1] = carry_val;
+            arrive1 = next_span;
+        } else if (lane == 0) {
+            y[carry_row] += carry_val;
         }
     }
-}
-
-// Adds the chunk heads/tails: the first entry of every run of equal rows sums the run.
-__global__ void __launch_bounds__(256) coo_fixup_kernel(const int* __restrict__ part_row, const float* __restrict__ part_val,
-                                                        int nparts, float* __restrict__ y)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nparts) return;
-    const int r = part_row[i];
-    if (i > 0 && part_row[i - 1] == r) return;
-    float acc = 0.0f;
-    for (int k = i; k < nparts && part_row[k] == r; k++) acc += part_val[k];
-    y[r] += acc;
+    if (arrive0 < 0 && arrive1 < 0) return;
+    __threadfence();
+    __syncwarp();
+    if (lane != 0) return;
+    const int arr[2] = {arrive0, arrive1};
+#pragma unroll
+    for (int q = 0; q < 2; q++) {
+        const int sp = arr[q];
+        if (sp < 0) continue;
+        const int4 d = __ldg(spans + sp);   // {row, first chunk, chunks, -}
+        if (atomicAdd(span_count + sp, 1) == d.z - 1) {
+            __threadfence();
+            float tot = __ldcg(part_val + 2 * d.y + 1);
+            for (int c = d.y + 1; c < d.y + d.z; c++) tot += __ldcg(part_val + 2 * c);
+            y[d.x] += tot;
+            span_count[sp] = 0;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------

@@ -28,10 +28,16 @@ def laplacian_2d(nx: int = 128):
 def _dedup_uniform_cols(rng, rows, cols, low, high):
     """Redraw columns until no row repeats one (uniform without replacement per row).
     rows must be sorted; low/high are per-entry inclusive/exclusive bounds."""
+    span = int(cols.max()) + 1 if low is None and cols.size else 0
     while True:
-        order = np.lexsort((cols, rows))
-        rows, cols = rows[order], cols[order]
-        if low is not None:
+        if low is None:
+            # one int64 key sort: the same order as lexsort((cols, rows)), equal keys are equal pairs
+            span = max(span, int(high))
+            key = np.sort(rows.astype(np.int64) * span + cols)
+            rows, cols = key // span, key % span
+        else:
+            order = np.lexsort((cols, rows))
+            rows, cols = rows[order], cols[order]
             low, high = low[order], high[order]
         dup = np.zeros(rows.size, bool)
         dup[1:] = (rows[1:] == rows[:-1]) & (cols[1:] == cols[:-1])
@@ -116,3 +122,47 @@ def csr_from_coo(height: int, row: np.ndarray):
     rp = np.zeros(height + 1, dtype=np.int64)
     np.cumsum(np.bincount(row, minlength=height), out=rp[1:])
     return rp.astype(np.int32)
+
+
+def laplacian_sq(nx: int, ny: int):
+    """L @ L for the 5-point Laplacian L on an nx-by-ny grid: the 13-point
+    squared-Laplacian stencil (20 on the diagonal, -8 to the four neighbours, 2 to
+    the four diagonal neighbours, 1 two steps along an axis, interior rows), the
+    Laplacian family at about 12 nonzeros per row."""
+    import scipy.sparse as sp
+
+    def lap1(k):
+        return sp.diags([-np.ones(k - 1), 2.0 * np.ones(k), -np.ones(k - 1)], [-1, 0, 1])
+
+    L = (sp.kron(sp.identity(ny), lap1(nx)) + sp.kron(lap1(ny), sp.identity(nx))).tocsr()
+    A = (L @ L).tocoo()
+    order = np.lexsort((A.col, A.row))
+    n = nx * ny
+    return n, n, A.row[order].astype(np.int32), A.col[order].astype(np.int32), A.data[order].astype(np.float32)
+
+
+BATCH_KINDS = ("laplacian", "zipf", "block")
+
+
+def batch_mixed(count: int = 512, lo: int = 1_000, hi: int = 200_000, seed: int = 0):
+    """Uneven batch: `count` matrices with row counts log-uniform in [lo, hi], each
+    drawn by seed from one of three generators at about 12 nonzeros per row --
+    the squared Laplacian (laplacian_sq on a near-square grid), Zipf(1.85) row
+    lengths clipped to [1, min(10000, n / 4)] (zipf_rows), or 3x3 blocks with block-row
+    degree uniform in [2, 6] (block_3x3, band +-2000 block columns).  Returns a list
+    of (kind, height, width, row, col, val)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        rows = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi)))))
+        kind = BATCH_KINDS[int(rng.integers(0, 3))]
+        s = int(rng.integers(0, 2**31 - 1))
+        if kind == "laplacian":
+            nx = max(3, int(np.sqrt(rows)))
+            ny = max(3, rows // nx)
+            out.append((kind,) + laplacian_sq(nx, ny))
+        elif kind == "zipf":
+            out.append((kind,) + zipf_rows(rows, s=1.85, max_len=min(10_000, max(1, rows // 4)), seed=s))
+        else:
+            out.append((kind,) + block_3x3(max(2, rows // 3), deg=(2, 6), band=2000, seed=s))
+    return out

@@ -405,6 +405,90 @@ int csp_adjoint_slots(csp_handle* h, size_t* nslots);
 int csp_adjoint_pattern(csp_handle* h, int* d_rows, int* d_cols);
 
 /* ------------------------------------------------------------------------ */
+/* Batched execution (no counterpart in the reference).  Many matrices of     */
+/* uneven size run in ONE persistent kernel over a (matrix, row-slice) work   */
+/* list: forward y_i += A_i x_i, adjoint xbar_i += A_i^T ybar_i and value      */
+/* gradients abar_i[s] = ybar_i[row(s)] * x_i[col(s)] over every stored slot.  */
+/* Each matrix is stored in the batch format chosen for it (format, slice     */
+/* height, block size): by the device autotuner, which times the candidates   */
+/* inside the persistent kernel and caches the decision per sparsity          */
+/* signature, by a byte-count model, or forced by the caller.  The batch takes */
+/* COO matrices (sorted copies are made when needed), not cocktails: it picks  */
+/* its own formats.  Vectors are concatenated in matrix order: x and xbar of   */
+/* length sum(width_i), y and ybar of sum(height_i), abar of the slots of all  */
+/* matrices; csp_batch_layout gives the offsets.  Results are deterministic.   */
+/* ------------------------------------------------------------------------ */
+typedef struct csp_batch csp_batch;
+
+#define CSP_BFMT_AUTO    (-1)
+#define CSP_BFMT_CSR      0  /* CSR in work blocks of <= 2040 entries, long rows chunked */
+#define CSP_BFMT_SELL32   1  /* sliced ELL, slice height 32                              */
+#define CSP_BFMT_SELL128  2  /* sliced ELL, slice height 128                             */
+#define CSP_BFMT_DIA      3  /* diagonals (at most 64)                                   */
+#define CSP_BFMT_BCSR2    4  /* 2x2 blocks                                               */
+#define CSP_BFMT_BCSR3    5  /* 3x3 blocks                                               */
+#define CSP_BFMT_BCSR4    6  /* 4x4 blocks                                               */
+#define CSP_BFMT_COUNT    7
+
+#define CSP_BATCH_TUNE_MODEL  0  /* fewest stored bytes among the feasible formats   */
+#define CSP_BATCH_TUNE_DEVICE 1  /* time the feasible formats in the persistent kernel */
+
+#define CSP_BATCH_FWD 1          /* y += A x                                        */
+#define CSP_BATCH_ADJ 2          /* xbar += A^T ybar and abar = ybar (x) x on A's slots */
+
+#define CSP_BV_X    0
+#define CSP_BV_Y    1
+#define CSP_BV_YBAR 2
+#define CSP_BV_XBAR 3
+#define CSP_BV_ABAR 4
+
+typedef struct csp_batch_opts {
+    int flags;               /* CSP_FLAG_BF16, CSP_FLAG_GRAPH, CSP_FLAG_ADJOINT (A^T and abar) */
+    int format;              /* CSP_BFMT_AUTO, or one format for every matrix (must be feasible) */
+    int tune;                /* CSP_BATCH_TUNE_MODEL or CSP_BATCH_TUNE_DEVICE (format AUTO)     */
+    const char* cache_path;  /* signature -> format decisions, appended; NULL: process cache only */
+} csp_batch_opts;
+
+/* Host-side structure of one matrix, as the format choice sees it. */
+typedef struct csp_batch_features {
+    int rows, cols, nnz, max_row;
+    int ndiag;                      /* distinct diagonals, -1 if more than 64 */
+    long long dia_slots;            /* ndiag * align(rows, 32)                */
+    long long sell_slots[2];        /* slice heights 32 and 128               */
+    long long bcsr_blocks[3];       /* block sizes 2, 3, 4                    */
+    unsigned int feasible;          /* bit f: format f is a candidate         */
+    int model_format;               /* the byte model's choice                */
+    unsigned long long signature;   /* sparsity signature (decision cache key) */
+} csp_batch_features;
+
+int csp_batch_features_of(const coo_matrix_if* mat, int flags, csp_batch_features* out);
+int csp_batch_create(const coo_matrix_if* const* mats, int n, const csp_batch_opts* opts, csp_batch** out);
+int csp_batch_free(csp_batch* b);
+/* n + 1 prefix offsets each (floats); any pointer may be NULL. */
+int csp_batch_layout(const csp_batch* b, long long* x_off, long long* y_off, long long* abar_off);
+int csp_batch_formats(const csp_batch* b, int* formats);
+int csp_batch_device_ptrs(const csp_batch* b, float** x, float** y, float** ybar, float** xbar, float** abar);
+/* Whole-vector copies on the batch stream: host `src` -> device, or device -> host
+ * `dst` (then synchronised).  Exactly one of src, dst is non-NULL. */
+int csp_batch_copy(csp_batch* b, int which, const float* src, float* dst);
+int csp_batch_set_stream(csp_batch* b, void* stream);   /* NULL: the batch's own stream */
+void* csp_batch_get_stream(const csp_batch* b);
+/* One persistent launch per repetition (a CUDA graph replay with CSP_FLAG_GRAPH). */
+int csp_batch_run(csp_batch* b, int what, int ntimes);
+/* The same work as per-matrix plain CSR launches (a CSR-vector SpMV per matrix
+ * and direction, one gradient kernel per matrix); needs every format CSR.  `lanes`
+ * per row: 1, 2, 4, 8, 16 or 32, or 0 for the power of two nearest below each
+ * matrix's mean row length. */
+int csp_batch_run_plain(csp_batch* b, int what, int ntimes, int lanes);
+int csp_batch_synchronize(csp_batch* b);
+/* Kernel launches one run (or one plain run) makes. */
+int csp_batch_launches(const csp_batch* b, int what, int plain);
+size_t csp_batch_device_bytes(const csp_batch* b);
+/* Row and column of every slot of matrix i (host arrays of abar_off[i+1]-abar_off[i]
+ * ints; row -1 for padding slots). */
+int csp_batch_pattern(const csp_batch* b, int i, int* rows, int* cols);
+
+/* ------------------------------------------------------------------------ */
 /* SpMV without device allocation.  No counterpart in the reference.          */
 /*                                                                            */
 /* For callers that cannot allocate device memory -- code running under a     */
