@@ -272,6 +272,32 @@ int Engine::build_adjoint(const cocktail_iif* mat)
             s.p0 = p.nnz;
             s.count = (size_t)p.nnz;
             break;
+        case PART_XPANEL: {
+            // slots follow the source part's own entry order (CSR or sorted COO), not
+            // the panel regrouping of the forward layout
+            std::vector<int> rows;
+            const int* cols;
+            if (p.from_csr) {
+                const csr_matrix_if& c = mat->csr;
+                rows.resize((size_t)c.matinfo.nnz);
+                for (int r = 0; r < c.matinfo.height; r++)
+                    for (int j = c.csr_row_ptr[r]; j < c.csr_row_ptr[r + 1]; j++) rows[j] = r;
+                cols = c.csr_col_id;
+            } else {
+                rows.assign(mat->coo.coo_row_id, mat->coo.coo_row_id + mat->coo.matinfo.nnz);
+                cols = mat->coo.coo_col_id;
+            }
+            int *d_r = nullptr, *d_c = nullptr;
+            if ((rc = upload_int(&d_r, rows.data(), rows.size(), std::max<size_t>(rows.size(), 1))) ||
+                (rc = upload_int(&d_c, cols, rows.size(), std::max<size_t>(rows.size(), 1))))
+                return rc;
+            s.kind = SEG_LIST;
+            s.a0 = d_r;
+            s.a1 = d_c;
+            s.p0 = (int)rows.size();
+            s.count = rows.size();
+            break;
+        }
         case PART_ELL:
             s.kind = SEG_ELL;
             s.a0 = p.i1;
@@ -311,7 +337,14 @@ int Engine::launch_abar(const float* ybar, float* abar, int* prow, int* pcol, cu
         int* pc = pcol ? pcol + s.offset : nullptr;
         const unsigned g = (unsigned)((s.count + 255) / 256);
         switch (s.kind) {
-        case SEG_DIA: abar_dia_kernel<<<g, 256, 0, st>>>(s.a0, s.p0, s.p1, s.p2, width, ybar, d_x, a, pr, pc); break;
+        case SEG_DIA:
+            if (a && s.p1 % 4 == 0 && (reinterpret_cast<uintptr_t>(a) & 15) == 0) {
+                const dim3 g4((unsigned)((s.p1 / 4 + 255) / 256), (unsigned)s.p0);
+                abar_dia4_kernel<<<g4, 256, 0, st>>>(s.a0, s.p1, s.p2, width, ybar, d_x, a);
+            } else {
+                abar_dia_kernel<<<g, 256, 0, st>>>(s.a0, s.p0, s.p1, s.p2, width, ybar, d_x, a, pr, pc);
+            }
+            break;
         case SEG_LIST: abar_list_kernel<<<g, 256, 0, st>>>(s.a0, s.a1, s.p0, ybar, d_x, a, pr, pc); break;
         case SEG_ELL: abar_ell_kernel<<<g, 256, 0, st>>>(s.a0, s.p0, s.p1, s.p2, ybar, d_x, a, pr, pc); break;
         case SEG_SELL: {

@@ -56,7 +56,7 @@ void info_of(const coo_matrix_if* m, cocktail_iif* c)
 }
 
 // ELL holding the first k entries of every row; the rest as CSR (adaptive kernel).
-int build_ell_split(const Coo& a, int k, cocktail_iif* c)
+int build_ell_split(const Coo& a, int k, int csr_meth, cocktail_iif* c)
 {
     const coo_matrix_if* m = a.m;
     const int h = m->matinfo.height;
@@ -101,14 +101,14 @@ int build_ell_split(const Coo& a, int k, cocktail_iif* c)
         memcpy(s.csr_col_id, rcol.data(), rcol.size() * sizeof(int));
         memcpy(s.csr_data, rval.data(), rval.size() * sizeof(float));
         c->ifusecsr = true;
-        c->csr_meth_num = 2;
+        c->csr_meth_num = csr_meth;
     }
     return CSP_OK;
 }
 
 // SELL (slices of sh rows) whose slice width is the q-quantile row length of the
 // slice; longer rows overflow to CSR (adaptive kernel).
-int build_sell_split(const Coo& a, int sh, double q, cocktail_iif* c)
+int build_sell_split(const Coo& a, int sh, double q, int csr_meth, cocktail_iif* c)
 {
     const coo_matrix_if* m = a.m;
     const int h = m->matinfo.height;
@@ -170,23 +170,23 @@ int build_sell_split(const Coo& a, int sh, double q, cocktail_iif* c)
         memcpy(s.csr_col_id, rcol.data(), rcol.size() * sizeof(int));
         memcpy(s.csr_data, rval.data(), rval.size() * sizeof(float));
         c->ifusecsr = true;
-        c->csr_meth_num = 2;
+        c->csr_meth_num = csr_meth;
     }
     return CSP_OK;
 }
 
 // Builds the candidate named `name` into c (fresh, zeroed).  Names: csr<m>, coo,
 // ell, sell<sh>, dia<m>, bdia<m>, bcsr<bh>x<bw>m<m>, bell<bh>x<bw>, sbell<bh>x<bw>,
-// ell<k>+csr2, sellq<sh>+csr2.
+// ell<k>+csr<m>, sellq<sh>+csr<m> (m = the overflow CSR part's kernel).  csr16 is the
+// x-panel kernel (CSP_METH_XPANEL).
 int build(const Coo& a, const std::string& name, cocktail_iif* c)
 {
     coo_matrix_if* m = const_cast<coo_matrix_if*>(a.m);
     csp_init_cocktail(c);
     info_of(m, c);
     int x = 0, y = 0, z = 0;
-    if (sscanf(name.c_str(), "ell%d+csr2", &x) == 1 && name.find('+') != std::string::npos)
-        return build_ell_split(a, x, c);
-    if (sscanf(name.c_str(), "sellq%d+csr2", &x) == 1) return build_sell_split(a, x, 0.75, c);
+    if (sscanf(name.c_str(), "ell%d+csr%d", &x, &y) == 2) return build_ell_split(a, x, y, c);
+    if (sscanf(name.c_str(), "sellq%d+csr%d", &x, &y) == 2) return build_sell_split(a, x, 0.75, y, c);
     if (sscanf(name.c_str(), "bcsr%dx%dm%d", &x, &y, &z) == 3) {
         c->ifusebcsr = true;
         c->bcsr_meth_num = z;
@@ -268,7 +268,7 @@ std::vector<std::string> candidates(const Coo& a)
     const int h = m->matinfo.height, w = m->matinfo.width;
     const long long nnz = m->matinfo.nnz;
     const double mean = h ? (double)nnz / h : 0.0;
-    std::vector<std::string> c = {"csr2", "coo"};
+    std::vector<std::string> c = {"csr2", "coo", "csr16"};
     if (mean >= 12.0) c.push_back("csr0");
     if (a.maxlen <= 64 && mean >= 2.0) c.push_back("csr3");
     // ELL / SELL when the padding stays below 1.5x / 2x of the nonzeros
@@ -288,8 +288,10 @@ std::vector<std::string> candidates(const Coo& a)
         for (int r = 0; r < h; r++) lens[r] = a.rp[r + 1] - a.rp[r];
         std::sort(lens.begin(), lens.end());
         const int k = lens.empty() ? 0 : lens[(size_t)(0.9 * (lens.size() - 1))];
-        if (k > 0 && k < a.maxlen) c.push_back("ell" + std::to_string(k) + "+csr2");
-        if (a.maxlen > 2 * mean + 1) c.push_back("sellq32+csr2");
+        for (const char* tail : {"+csr2", "+csr16"}) {
+            if (k > 0 && k < a.maxlen) c.push_back("ell" + std::to_string(k) + tail);
+            if (a.maxlen > 2 * mean + 1) c.push_back(std::string("sellq32") + tail);
+        }
     }
     if (h == w && nnz > 0) {
         // DIA only if the padded storage stays within the reference's 2x rule; probed by conversion

@@ -25,6 +25,7 @@
 #include "kernels/diag.cuh"
 #include "kernels/block.cuh"
 #include "kernels/spmm.cuh"
+#include "kernels/xpanel.cuh"
 
 namespace csp {
 
@@ -176,6 +177,13 @@ int Engine::add_csr(const csr_matrix_if& c, int method)
     int rc;
     if ((rc = check_row_ptr(c.csr_row_ptr, m, "CSR part")) || (rc = check_ids(c.csr_col_id, nnz, width, "CSR part")))
         return rc;
+    if (method == CSP_METH_XPANEL) {
+        if (nrhs > 1) return set_error(CSP_EUNSUP, "x-panel CSR part with several right-hand sides");
+        std::vector<int> rows((size_t)nnz);
+        for (int r = 0; r < m; r++)
+            for (int j = c.csr_row_ptr[r]; j < c.csr_row_ptr[r + 1]; j++) rows[j] = r;
+        return add_xpanel(rows.data(), c.csr_col_id, c.csr_data, nnz, true);
+    }
     Part p;
     p.kind = PART_CSR;
     p.method = method;
@@ -225,7 +233,7 @@ int Engine::add_csr(const csr_matrix_if& c, int method)
     return CSP_OK;
 }
 
-int Engine::add_coo(const coo_matrix_if& c)
+int Engine::add_coo(const coo_matrix_if& c, int method)
 {
     const int nnz = c.matinfo.nnz;
     if (nnz < 0 || (nnz > 0 && (!c.coo_row_id || !c.coo_col_id || !c.coo_data)))
@@ -236,6 +244,7 @@ int Engine::add_coo(const coo_matrix_if& c)
     for (int i = 0; i < nnz; i++)
         if (c.coo_row_id[i] < 0 || c.coo_row_id[i] >= height || c.coo_col_id[i] < 0 || c.coo_col_id[i] >= width)
             return set_error(CSP_EINVAL, "COO part: entry %d out of range", i);
+    if (method == CSP_METH_XPANEL) return add_xpanel(c.coo_row_id, c.coo_col_id, c.coo_data, nnz, false);
     Part p;
     p.kind = PART_COO;
     p.method = 0;
@@ -271,6 +280,121 @@ int Engine::add_coo(const coo_matrix_if& c)
         return rc;
     if (!spans.empty()) CSP_CUDA(cudaMemcpy(p.spans, spans.data(), spans.size() * sizeof(int4), cudaMemcpyHostToDevice));
     CSP_CUDA(cudaMemset(p.scratch_row, 0, ns * sizeof(int)));   // arrival counters
+    parts.push_back(p);
+    return CSP_OK;
+}
+
+// x-panel layout (kernels/xpanel.cuh) of nnz entries sorted by row, indices already
+// validated.  Entries are regrouped by column panel (stable, so rows stay sorted inside
+// a panel), each panel padded to whole tiles; runs of one row inside a tile get slots
+// numbered row by row, in panel order inside a row.
+int Engine::add_xpanel(const int* rows, const int* cols, const float* vals, int nnz, bool from_csr)
+{
+    using dev::kXpTile;
+    if (nnz == 0) return CSP_OK;
+    Part p;
+    p.kind = PART_XPANEL;
+    p.method = CSP_METH_XPANEL;
+    p.nnz = nnz;
+    p.from_csr = from_csr;
+    // the widest panel that fits beside the tile rings in one CTA's shared memory
+    int dev_id = 0, optin = 0, sms = 0;
+    CSP_CUDA(cudaGetDevice(&dev_id));
+    CSP_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev_id));
+    CSP_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev_id));
+    const size_t ring = bf16 ? dev::xpanel_ring_bytes<__nv_bfloat16>() : dev::xpanel_ring_bytes<float>();
+    const long long room = ((long long)optin - (long long)ring) / 4 / 64 * 64;
+    if (room < 64) return set_error(CSP_EUNSUP, "x-panel part: %d bytes of shared memory per block are too few", optin);
+    p.panel_w = (int)std::min<long long>({room, dev::kXpPanelMax, pad_to(std::max(width, 1), 4)});
+    const int P = (width + p.panel_w - 1) / p.panel_w;
+    p.npanels = P;
+    // stable counting sort by panel
+    std::vector<long long> cnt((size_t)P + 1, 0);
+    for (int i = 0; i < nnz; i++) cnt[(size_t)cols[i] / p.panel_w + 1]++;
+    std::vector<int> tile0((size_t)P + 1, 0);
+    for (int q = 0; q < P; q++) {
+        const long long t = tile0[q] + (cnt[q + 1] + kXpTile - 1) / kXpTile;
+        if (t >= INT32_MAX / kXpTile) return set_error(CSP_EUNSUP, "x-panel part: too many entries");
+        tile0[q + 1] = (int)t;
+    }
+    for (int q = 0; q < P; q++) cnt[q + 1] += cnt[q];
+    std::vector<int> order((size_t)nnz);
+    {
+        std::vector<long long> next(cnt.begin(), cnt.end() - 1);
+        for (int i = 0; i < nnz; i++) order[(size_t)next[(size_t)cols[i] / p.panel_w]++] = i;
+    }
+    const int T = tile0[P];
+    const size_t slots_len = (size_t)T * kXpTile;
+    // a run starts at every tile start and every row change
+    auto starts_run = [&](long long j, long long b) {
+        return (j - b) % kXpTile == 0 || rows[order[(size_t)j - 1]] != rows[order[(size_t)j]];
+    };
+    std::vector<int> nruns((size_t)height, 0);
+    for (int q = 0; q < P; q++)
+        for (long long j = cnt[q]; j < cnt[q + 1]; j++)
+            if (starts_run(j, cnt[q])) nruns[rows[order[(size_t)j]]]++;
+    // listed rows (rows with entries) and their slot ranges
+    std::vector<int> run_ptr, run_rows;
+    std::vector<long long> first((size_t)height, -1);
+    run_ptr.push_back(0);
+    long long total = 0;
+    for (int r = 0; r < height; r++) {
+        if (!nruns[r]) continue;
+        first[r] = total;
+        total += nruns[r];
+        run_rows.push_back(r);
+        run_ptr.push_back((int)total);
+    }
+    if (total >= INT32_MAX) return set_error(CSP_EUNSUP, "x-panel part: too many runs");
+    // per-entry slots, panel-local columns and values in tile order
+    std::vector<int> slot(slots_len, 0);
+    std::vector<unsigned short> lcol(slots_len, 0);
+    std::vector<float> val(slots_len, 0.0f);
+    for (int q = 0; q < P; q++) {
+        const long long b = cnt[q], e = cnt[q + 1];
+        const size_t o = (size_t)tile0[q] * kXpTile;
+        int cur = 0;
+        for (long long j = b; j < e; j++) {
+            const int i = order[(size_t)j];
+            if (starts_run(j, b)) cur = (int)(first[rows[i]]++);
+            slot[o + (size_t)(j - b)] = cur;
+            lcol[o + (size_t)(j - b)] = (unsigned short)(cols[i] - q * p.panel_w);
+            val[o + (size_t)(j - b)] = vals[i];
+        }
+        // pad entries extend the panel's last run (0 * x[panel start])
+        for (long long j = e - b; j % kXpTile != 0; j++) slot[o + (size_t)j] = cur;
+    }
+    p.ntiles = T;
+    p.nrun_rows = (int)run_rows.size();
+    const bool all_rows = p.nrun_rows == height;
+    // listed rows with many slots, merged by a lane group each
+    std::vector<int> long_list;
+    for (int i = 0; i < p.nrun_rows; i++)
+        if (run_ptr[i + 1] - run_ptr[i] > dev::kXpShortRuns) long_list.push_back(i);
+    p.nlong = (int)long_list.size();
+
+    int rc;
+    if ((rc = upload_int(&p.i0, slot.data(), slots_len, slots_len)) ||
+        (rc = upload_val(&p.v, val.data(), slots_len, slots_len)) ||
+        (rc = alloc(reinterpret_cast<void**>(&p.lcol), slots_len * sizeof(unsigned short))) ||
+        (rc = upload_int(&p.tile0, tile0.data(), tile0.size(), tile0.size())) ||
+        (rc = upload_int(&p.run_ptr, run_ptr.data(), run_ptr.size(), run_ptr.size())) ||
+        (rc = alloc(reinterpret_cast<void**>(&p.partial), (size_t)total * sizeof(float))))
+        return rc;
+    CSP_CUDA(cudaMemcpy(p.lcol, lcol.data(), slots_len * sizeof(unsigned short), cudaMemcpyHostToDevice));
+    if (!all_rows && (rc = upload_int(&p.run_rows, run_rows.data(), run_rows.size(), run_rows.size()))) return rc;
+    if ((rc = upload_int(&p.long_list, long_list.data(), long_list.size(), std::max<size_t>(long_list.size(), 1)))) return rc;
+    // grid: as many CTAs as fit on the device at once, but no more than the tiles need:
+    // each CTA's entries should outweigh the x panel it copies
+    p.smem = (size_t)p.panel_w * sizeof(float) + ring;
+    auto kern = bf16 ? reinterpret_cast<const void*>(&dev::xpanel_kernel<__nv_bfloat16>)
+                     : reinterpret_cast<const void*>(&dev::xpanel_kernel<float>);
+    CSP_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem));
+    int per_sm = 0;
+    CSP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, dev::kXpThreads, p.smem));
+    const long long resident = (long long)sms * std::max(per_sm, 1);
+    const long long by_work = std::max<long long>(1, (long long)slots_len * 10 / (long long)(p.panel_w * 4));
+    p.ncta = (int)std::max<long long>(1, std::min({resident, by_work, (long long)T}));
     parts.push_back(p);
     return CSP_OK;
 }
@@ -648,6 +772,14 @@ static void launch_part(const Part& p, const float* x, float* y, int n, cudaStre
 #undef CSP_BCSR
         break;
     }
+    case PART_XPANEL: {
+        dev::xpanel_kernel<V><<<p.ncta, kXpThreads, p.smem, st>>>(
+            p.tile0, p.ntiles, p.npanels, p.i0, p.lcol, v, x, n, p.panel_w, p.partial);
+        const long long mthreads = (long long)grid_for(p.nrun_rows, 256) * 256 + (long long)p.nlong * kXpMergeLanes;
+        xpanel_merge_kernel<<<grid_for(mthreads, 256), 256, 0, st>>>(p.run_ptr, p.run_rows, p.nrun_rows, p.long_list,
+                                                                     p.nlong, p.partial, y);
+        break;
+    }
     case PART_GBCSR: {
         if (p.nbr == 0) return;
         const unsigned g = grid_for((long long)p.nbr * 8, 256);
@@ -664,7 +796,9 @@ static void launch_part(const Part& p, const float* x, float* y, int n, cudaStre
 
 int Engine::launches_per_spmv() const
 {
-    return (int)parts.size();
+    int n = 0;
+    for (const Part& p : parts) n += p.kind == PART_XPANEL ? 2 : 1;
+    return n;
 }
 
 int Engine::enqueue_parts(const std::vector<Part>& ps, const float* x, float* y, int n, cudaStream_t st)
@@ -762,7 +896,7 @@ int Engine::init(const cocktail_iif* mat, const float* vec, const float* res, in
     if (mat->ifusesell && (rc = add_sell(mat->sell, mat->sell_meth_num))) return rc;
     if (mat->ifuseell && (rc = add_ell(mat->ell, mat->ell_meth_num))) return rc;
     if (mat->ifusecsr && (rc = add_csr(mat->csr, mat->csr_meth_num))) return rc;
-    if (mat->ifusecoo && (rc = add_coo(mat->coo))) return rc;
+    if (mat->ifusecoo && (rc = add_coo(mat->coo, mat->coo_meth_num))) return rc;
     if ((flags & CSP_FLAG_ADJOINT) && (rc = build_adjoint(mat))) return rc;
     CSP_CUDA(cudaDeviceSynchronize());
     return CSP_OK;

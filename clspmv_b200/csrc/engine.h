@@ -11,7 +11,8 @@
 
 namespace csp {
 
-enum PartKind { PART_BDIA, PART_DIA, PART_SBELL, PART_BELL, PART_BCSR, PART_SELL, PART_ELL, PART_CSR, PART_COO, PART_GBCSR };
+enum PartKind { PART_BDIA, PART_DIA, PART_SBELL, PART_BELL, PART_BCSR, PART_SELL, PART_ELL, PART_CSR, PART_COO, PART_GBCSR,
+                PART_XPANEL };
 
 // One uploaded sub-matrix and its launch parameters.
 struct Part {
@@ -36,6 +37,16 @@ struct Part {
     int group = 0;    // CSR sub-warp lanes per row
     int nblocks = 0;  // CSR adaptive row blocks
     int npad = 0, nwarps = 0;  // COO
+    // x-panel layout (kernels/xpanel.cuh): i0 = run slot per entry, v = values
+    unsigned short* lcol = nullptr;   // column inside the entry's panel
+    int* tile0 = nullptr;             // first tile of each panel (npanels + 1)
+    int* run_ptr = nullptr;           // slots of each listed row (nrun_rows + 1)
+    int* run_rows = nullptr;          // listed rows: rows with entries, or null when all have some
+    int* long_list = nullptr;         // listed rows with more than kXpShortRuns slots (nlong)
+    float* partial = nullptr;         // one sum per run
+    int ntiles = 0, npanels = 0, panel_w = 0, nrun_rows = 0, ncta = 0, nlong = 0;
+    size_t smem = 0;                  // dynamic shared memory of the x-panel kernel
+    bool from_csr = false;            // adjoint: value-gradient order follows the CSR part
 };
 
 enum SegKind { SEG_NONE, SEG_DIA, SEG_LIST, SEG_ELL, SEG_SELL };
@@ -87,7 +98,8 @@ struct Engine {
     int upload_val(void** d, const float* h, size_t n, size_t cap);
 
     int add_csr(const csr_matrix_if& c, int method);
-    int add_coo(const coo_matrix_if& c);
+    int add_coo(const coo_matrix_if& c, int method);
+    int add_xpanel(const int* rows, const int* cols, const float* vals, int nnz, bool from_csr);
     int add_ell(const ell_matrix_if& e, int method);
     int add_sell(const sell_matrix_if& s, int method);
     int add_dia(const dia_matrix_iif& d, int method);

@@ -38,6 +38,26 @@ __global__ void __launch_bounds__(256) abar_dia_kernel(const int* __restrict__ o
     put_slot(i, in ? r : -1, c, ybar, x, abar, prow, pcol);
 }
 
+// Value gradients of DIA-layout slots, four rows per thread and one diagonal per
+// grid row (blockIdx.y): no 64-bit index division, one 128-bit store per thread.
+// len is a multiple of 4 and abar + d * len is 16-byte aligned (checked by the host).
+__global__ void __launch_bounds__(256) abar_dia4_kernel(const int* __restrict__ off, int len, int m, int n,
+                                                        const float* __restrict__ ybar, const float* __restrict__ x,
+                                                        float* __restrict__ abar)
+{
+    const int r = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
+    if (r >= len) return;
+    const int d = blockIdx.y;
+    const int o = __ldg(off + d);
+    float g[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int rr = r + q, c = rr + o;
+        g[q] = (rr < m && c >= 0 && c < n) ? __ldg(ybar + rr) * __ldg(x + c) : 0.0f;
+    }
+    __stcs(reinterpret_cast<float4*>(abar + (size_t)d * len + r), make_float4(g[0], g[1], g[2], g[3]));
+}
+
 // Entry lists with explicit row ids (COO; CSR with its row-id array).
 __global__ void __launch_bounds__(256) abar_list_kernel(const int* __restrict__ rows, const int* __restrict__ cols, int nnz,
                                                         const float* __restrict__ ybar, const float* __restrict__ x,

@@ -311,6 +311,16 @@ typedef struct csp_handle csp_handle;
 #define CSP_FLAG_GRAPH     0x4  /* replay do_spmv as one captured CUDA graph                                   */
 #define CSP_FLAG_ADJOINT   0x8  /* also build the transposed structures for csp_spmv_adjoint                  */
 
+/* Kernel choice for a CSR or COO sub-matrix (csr_meth_num / coo_meth_num; no
+ * counterpart in the reference): x staged in shared memory by column panels of at
+ * most 32,768 columns.  The sub-matrix's nonzeros are regrouped by panel; each CTA
+ * copies its panels of x into shared memory and reduces 128-entry tiles to one
+ * partial sum per run of one row, and a second kernel adds every row's partials to
+ * res in panel order (deterministic, two launches per SpMV).  Meant for matrices
+ * whose column indices have no locality (random graphs), where gathering x from
+ * global memory is bound by L2 request throughput.  One right-hand side only. */
+#define CSP_METH_XPANEL    16
+
 /* Upload every used sub-matrix of `mat`, x = vec (length mat_width) and
  * res (length mat_height; may be NULL for zeros), and select one kernel per
  * sub-matrix from its *_meth_num.  (spmv_cocktail.cpp:1593 init_mat_kernels) */

@@ -26,7 +26,7 @@ CASES = {
     "rect_tall": SMALL["rect_tall"],
     "lap_noise": _plus_noise(M.laplacian_2d(96), 3000, 2),
 }
-VARIANTS = [("dia", 1), ("bdia", 1), ("csr", 2), ("coo", 0), ("ell", 1), ("sell", 0),
+VARIANTS = [("dia", 1), ("bdia", 1), ("csr", 2), ("coo", 0), ("csr", 16), ("coo", 16), ("ell", 1), ("sell", 0),
             ("bcsr", 0), ("sbell", 0), ("bell", 0)]
 
 

@@ -24,7 +24,7 @@ CASES = {
     "stencil": M.stencil_27(20, seed=62),
     "block4": M.block_3x3(3000, deg=(4, 10), band=50, seed=63, bs=4),
 }
-VARIANTS = [("csr", 2, {}), ("csr", 0, {}), ("coo", 0, {}), ("ell", 1, {}), ("sell", 0, {}), ("dia", 1, {}),
+VARIANTS = [("csr", 2, {}), ("csr", 0, {}), ("coo", 0, {}), ("csr", 16, {}), ("coo", 16, {}), ("ell", 1, {}), ("sell", 0, {}), ("dia", 1, {}),
             ("bdia", 1, {}), ("bdia", 0, {}), ("bcsr", 0, {"bwidth": 4, "bheight": 4}),
             ("bell", 0, {"bwidth": 4, "bheight": 4}), ("sbell", 0, {"bwidth": 4, "bheight": 4})]
 

@@ -34,6 +34,7 @@ ALL = {**CASES, **MEDIUM}
 VARIANTS = (
     [("csr", m, {}) for m in range(7)]
     + [("coo", 0, {})]
+    + [("csr", 16, {}), ("coo", 16, {})]
     + [("ell", m, {}) for m in (0, 1)]
     + [("sell", 0, {"slice_height": 32}), ("sell", 1, {"slice_height": 128}), ("sell", 2, {"slice_height": 32}),
        ("sell", 0, {"slice_height": 5})]
@@ -89,7 +90,7 @@ def test_diagonal(name, variant):
     check(case, y, x, y0)
 
 
-@pytest.mark.parametrize("fmt,method", [("csr", 2), ("coo", 0), ("sell", 0), ("csr", 0)])
+@pytest.mark.parametrize("fmt,method", [("csr", 2), ("coo", 0), ("sell", 0), ("csr", 0), ("csr", 16), ("coo", 16)])
 def test_accumulates_over_repeated_spmv(fmt, method):
     """do_spmv(3) computes y0 + 3*A*x (the reference's accumulate semantics)."""
     case = MEDIUM["zipf_100k"]
