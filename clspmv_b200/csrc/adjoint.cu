@@ -339,8 +339,8 @@ int Engine::launch_abar(const float* ybar, float* abar, int* prow, int* pcol, cu
         switch (s.kind) {
         case SEG_DIA:
             if (a && s.p1 % 4 == 0 && (reinterpret_cast<uintptr_t>(a) & 15) == 0) {
-                const dim3 g4((unsigned)((s.p1 / 4 + 255) / 256), (unsigned)s.p0);
-                abar_dia4_kernel<<<g4, 256, 0, st>>>(s.a0, s.p1, s.p2, width, ybar, d_x, a);
+                const unsigned g4 = (unsigned)((s.p1 / 4 + 255) / 256);
+                abar_dia4_kernel<<<g4, 256, (size_t)s.p0 * sizeof(int), st>>>(s.a0, s.p0, s.p1, s.p2, width, ybar, d_x, a);
             } else {
                 abar_dia_kernel<<<g, 256, 0, st>>>(s.a0, s.p0, s.p1, s.p2, width, ybar, d_x, a, pr, pc);
             }

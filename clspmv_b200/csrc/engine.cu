@@ -602,9 +602,31 @@ int Engine::add_generic_bcsr(const bcsr_matrix_if& b, int method)
     if (b.bcsr_row_ptr[b.bcsr_row_num] > b.bcsr_block_num) return set_error(CSP_EINVAL, "generic BCSR: row pointer past the blocks");
     if ((rc = check_ids(b.bcsr_col_id, (size_t)b.bcsr_block_num, width, "generic BCSR"))) return rc;
     if ((rc = upload_int(&p.i0, b.bcsr_row_ptr, (size_t)b.bcsr_row_num + 1, (size_t)b.bcsr_row_num + 1)) ||
-        (rc = upload_int(&p.i1, b.bcsr_col_id, b.bcsr_block_num, b.bcsr_block_num)) ||
+        (rc = upload_int(&p.i1, b.bcsr_col_id, b.bcsr_block_num, (size_t)pad_to(b.bcsr_block_num, 4) + 4)) ||
         (rc = upload_val(&p.v, b.bcsr_data, nd, nd)))
         return rc;
+    // one right-hand side, blocks of at most 16 elements: work items of whole block rows
+    // for the adaptive kernel (kernels/block.cuh bcsr_adaptive_kernel), unless a block
+    // row is too long for one CTA or the planes' stride is not a multiple of 4
+    if (nrhs == 1 && bw * bh <= 16 && b.bcsr_aligned_size % 4 == 0) {
+        std::vector<int4> work;
+        const int* rp = b.bcsr_row_ptr;
+        bool fits = true;
+        int r0 = 0;
+        for (int r = 0; r < p.nbr && fits; r++) {
+            if (rp[r + 1] - rp[r] > dev::kGbBlocks - 3) fits = false;
+            else if (r - r0 == dev::kGbRows || rp[r + 1] - rp[r0] > dev::kGbBlocks - 3) {
+                work.push_back(make_int4(r0, r - r0, rp[r0], rp[r]));
+                r0 = r;
+            }
+        }
+        if (fits && p.nbr > r0) work.push_back(make_int4(r0, p.nbr - r0, rp[r0], rp[p.nbr]));
+        if (fits && !work.empty()) {
+            if ((rc = alloc(reinterpret_cast<void**>(&p.blocks), work.size() * sizeof(int4)))) return rc;
+            CSP_CUDA(cudaMemcpy(p.blocks, work.data(), work.size() * sizeof(int4), cudaMemcpyHostToDevice));
+            p.nblocks = (int)work.size();
+        }
+    }
     parts.push_back(p);
     return CSP_OK;
 }
@@ -782,6 +804,15 @@ static void launch_part(const Part& p, const float* x, float* y, int n, cudaStre
     }
     case PART_GBCSR: {
         if (p.nbr == 0) return;
+        if (p.nblocks > 0) {
+#define CSP_GBA(BH, BW) bcsr_adaptive_kernel<V, BH, BW><<<p.nblocks, kGbThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.blocks, p.stride, p.m, n)
+            switch (p.bh * 10 + p.bw) {
+            case 11: CSP_GBA(1, 1); break; case 22: CSP_GBA(2, 2); break; case 33: CSP_GBA(3, 3); break;
+            case 44: CSP_GBA(4, 4); break;
+            }
+#undef CSP_GBA
+            return;
+        }
         const unsigned g = grid_for((long long)p.nbr * 8, 256);
 #define CSP_GB(BH, BW) bcsr_generic_kernel<V, BH, BW, 8><<<g, 256, 0, st>>>(p.i0, p.i1, v, x, y, p.nbr, p.stride, p.m, n)
         switch (p.bh * 10 + p.bw) {

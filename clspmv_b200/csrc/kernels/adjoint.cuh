@@ -38,24 +38,34 @@ __global__ void __launch_bounds__(256) abar_dia_kernel(const int* __restrict__ o
     put_slot(i, in ? r : -1, c, ybar, x, abar, prow, pcol);
 }
 
-// Value gradients of DIA-layout slots, four rows per thread and one diagonal per
-// grid row (blockIdx.y): no 64-bit index division, one 128-bit store per thread.
-// len is a multiple of 4 and abar + d * len is 16-byte aligned (checked by the host).
-__global__ void __launch_bounds__(256) abar_dia4_kernel(const int* __restrict__ off, int len, int m, int n,
+// Value gradients of DIA-layout slots, four rows per thread over every diagonal: the
+// thread's ybar values are loaded once, x is read around row r + off[d] (neighbouring
+// threads share those lines in L1), and each diagonal gets one 128-bit streaming store,
+// so a warp writes 512 contiguous bytes per diagonal.  No 64-bit index division.
+// len is a multiple of 4 and abar is 16-byte aligned (checked by the host); the
+// offsets (nd of them) are staged in shared memory.
+__global__ void __launch_bounds__(256) abar_dia4_kernel(const int* __restrict__ off, int nd, int len, int m, int n,
                                                         const float* __restrict__ ybar, const float* __restrict__ x,
                                                         float* __restrict__ abar)
 {
+    extern __shared__ int s_off[];
+    for (int i = threadIdx.x; i < nd; i += blockDim.x) s_off[i] = __ldg(off + i);
+    __syncthreads();
     const int r = 4 * (blockIdx.x * blockDim.x + threadIdx.x);
     if (r >= len) return;
-    const int d = blockIdx.y;
-    const int o = __ldg(off + d);
-    float g[4];
+    float yb[4];
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-        const int rr = r + q, c = rr + o;
-        g[q] = (rr < m && c >= 0 && c < n) ? __ldg(ybar + rr) * __ldg(x + c) : 0.0f;
+    for (int q = 0; q < 4; q++) yb[q] = r + q < m ? __ldg(ybar + r + q) : 0.0f;
+    for (int d = 0; d < nd; d++) {
+        const int o = s_off[d];
+        float g[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int c = r + q + o;
+            g[q] = (c >= 0 && c < n) ? yb[q] * __ldg(x + c) : 0.0f;
+        }
+        __stcs(reinterpret_cast<float4*>(abar + (size_t)d * len + r), make_float4(g[0], g[1], g[2], g[3]));
     }
-    __stcs(reinterpret_cast<float4*>(abar + (size_t)d * len + r), make_float4(g[0], g[1], g[2], g[3]));
 }
 
 // Entry lists with explicit row ids (COO; CSR with its row-id array).

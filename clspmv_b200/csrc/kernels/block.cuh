@@ -142,5 +142,93 @@ __global__ void __launch_bounds__(256) bcsr_generic_kernel(const int* __restrict
     }
 }
 
+// Generic BCSR, one right-hand side, for blocks of at most 16 elements: the host cuts
+// the block rows into work items {first block row, block rows, first block, end block}
+// of at most kGbBlocks - 3 blocks and kGbRows block rows.  Each thread loads four
+// consecutive blocks -- one 128-bit load of their column ids and one per block element
+// plane, so every matrix byte moves in a coalesced 128-bit load -- and leaves each
+// block's BH row products in shared memory; then a lane group per block row adds its
+// blocks in order (fixed shuffle tree) and updates y.  Requires the block planes'
+// stride (`aligned`) to be a multiple of 4 and the column ids padded to a multiple of 4.
+constexpr int kGbThreads = 256;
+constexpr int kGbBlocks = 4 * kGbThreads;
+constexpr int kGbRows = 256;
+
+template <int BH, int G>
+__device__ __forceinline__ void gb_rows(const int* s_rp, const float* prod, int br0, int nrows, int m,
+                                        float* __restrict__ y)
+{
+    const int lane = threadIdx.x % G;
+    constexpr int ngroups = kGbThreads / G;
+    for (int first = 0; first < nrows; first += ngroups) {
+        const int lr = first + threadIdx.x / G;
+        const bool valid = lr < nrows;
+        const int a = valid ? s_rp[lr] : 0, b = valid ? s_rp[lr + 1] : 0;
+        float acc[BH];
+#pragma unroll
+        for (int h = 0; h < BH; h++) acc[h] = 0.0f;
+        for (int k = a + lane; k < b; k += G)
+#pragma unroll
+            for (int h = 0; h < BH; h++) acc[h] += prod[k * BH + h];
+#pragma unroll
+        for (int h = 0; h < BH; h++) {
+            const float t = group_sum<G>(acc[h]);
+            const int r = (br0 + lr) * BH + h;
+            if (valid && lane == 0 && r < m) y[r] += t;
+        }
+    }
+}
+
+template <class V, int BH, int BW>
+__global__ void __launch_bounds__(kGbThreads) bcsr_adaptive_kernel(const int* __restrict__ rp, const int* __restrict__ col,
+                                                                   const V* __restrict__ data, const float* __restrict__ x,
+                                                                   float* __restrict__ y, const int4* __restrict__ work,
+                                                                   int aligned, int m, int n)
+{
+    __shared__ float prod[kGbBlocks * BH];
+    __shared__ int s_rp[kGbRows + 1];
+    const int4 wk = __ldg(work + blockIdx.x);
+    const int br0 = wk.x, nrows = wk.y, s = wk.z, e = wk.w;
+    const int s4 = s & ~3;
+    const int tid = threadIdx.x;
+    const int j = s4 + 4 * tid;
+    const bool act = j < e;
+    int4 c = make_int4(0, 0, 0, 0);
+    float4 d[BH * BW];
+    if (act) {
+        c = ld_int4(col + j);
+#pragma unroll
+        for (int k = 0; k < BH * BW; k++) d[k] = Val<V>::ld4(data + (size_t)k * aligned + j);
+    }
+    if (tid < nrows) s_rp[tid] = __ldg(rp + br0 + tid) - s4;
+    if (tid == 0) s_rp[nrows] = e - s4;
+    if (act) {
+        const int cc[4] = {c.x, c.y, c.z, c.w};
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const bool in = j + q >= s && j + q < e;
+            float xv[BW];
+#pragma unroll
+            for (int w = 0; w < BW; w++) xv[w] = (in && cc[q] + w < n) ? __ldg(x + cc[q] + w) : 0.0f;
+#pragma unroll
+            for (int h = 0; h < BH; h++) {
+                float t = 0.0f;
+#pragma unroll
+                for (int w = 0; w < BW; w++) {
+                    const float4 v = d[h * BW + w];
+                    const float a = q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w;
+                    t += a * xv[w];
+                }
+                prod[(4 * tid + q) * BH + h] = in ? t : 0.0f;
+            }
+        }
+    }
+    __syncthreads();
+    if (nrows * 32 <= kGbThreads * 2) gb_rows<BH, 32>(s_rp, prod, br0, nrows, m, y);
+    else if (nrows * 8 <= kGbThreads * 2) gb_rows<BH, 8>(s_rp, prod, br0, nrows, m, y);
+    else if (nrows * 2 <= kGbThreads * 2) gb_rows<BH, 2>(s_rp, prod, br0, nrows, m, y);
+    else gb_rows<BH, 1>(s_rp, prod, br0, nrows, m, y);
+}
+
 }  // namespace dev
 }  // namespace csp
