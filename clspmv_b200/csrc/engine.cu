@@ -601,17 +601,14 @@ int Engine::add_generic_bcsr(const bcsr_matrix_if& b, int method)
     if ((rc = check_row_ptr(b.bcsr_row_ptr, b.bcsr_row_num, "generic BCSR"))) return rc;
     if (b.bcsr_row_ptr[b.bcsr_row_num] > b.bcsr_block_num) return set_error(CSP_EINVAL, "generic BCSR: row pointer past the blocks");
     if ((rc = check_ids(b.bcsr_col_id, (size_t)b.bcsr_block_num, width, "generic BCSR"))) return rc;
-    if ((rc = upload_int(&p.i0, b.bcsr_row_ptr, (size_t)b.bcsr_row_num + 1, (size_t)b.bcsr_row_num + 1)) ||
-        (rc = upload_int(&p.i1, b.bcsr_col_id, b.bcsr_block_num, (size_t)pad_to(b.bcsr_block_num, 4) + 4)) ||
-        (rc = upload_val(&p.v, b.bcsr_data, nd, nd)))
-        return rc;
+    if ((rc = upload_int(&p.i0, b.bcsr_row_ptr, (size_t)b.bcsr_row_num + 1, (size_t)b.bcsr_row_num + 1))) return rc;
     // one right-hand side, blocks of at most 16 elements: work items of whole block rows
     // for the adaptive kernel (kernels/block.cuh bcsr_adaptive_kernel), unless a block
     // row is too long for one CTA or the planes' stride is not a multiple of 4
-    if (nrhs == 1 && bw * bh <= 16 && b.bcsr_aligned_size % 4 == 0) {
-        std::vector<int4> work;
+    std::vector<int4> work;
+    bool fits = nrhs == 1 && bw * bh <= 16 && b.bcsr_aligned_size % 4 == 0;
+    if (fits) {
         const int* rp = b.bcsr_row_ptr;
-        bool fits = true;
         int r0 = 0;
         for (int r = 0; r < p.nbr && fits; r++) {
             if (rp[r + 1] - rp[r] > dev::kGbBlocks - 3) fits = false;
@@ -621,11 +618,40 @@ int Engine::add_generic_bcsr(const bcsr_matrix_if& b, int method)
             }
         }
         if (fits && p.nbr > r0) work.push_back(make_int4(r0, p.nbr - r0, rp[r0], rp[p.nbr]));
-        if (fits && !work.empty()) {
-            if ((rc = alloc(reinterpret_cast<void**>(&p.blocks), work.size() * sizeof(int4)))) return rc;
-            CSP_CUDA(cudaMemcpy(p.blocks, work.data(), work.size() * sizeof(int4), cudaMemcpyHostToDevice));
-            p.nblocks = (int)work.size();
+        fits = fits && !work.empty();
+    }
+    const int nblk = b.bcsr_block_num;
+    if (!fits) {
+        if ((rc = upload_int(&p.i1, b.bcsr_col_id, nblk, (size_t)pad_to(nblk, 4) + 4)) ||
+            (rc = upload_val(&p.v, b.bcsr_data, nd, nd)))
+            return rc;
+    } else {
+        // inside each item, blocks in column order (stable); tgt = row-order position - (s & ~3)
+        std::vector<int> perm((size_t)nblk), col((size_t)pad_to(nblk, 4) + 4, 0);
+        std::vector<unsigned short> tgt(col.size(), 0);
+        for (int k = 0; k < nblk; k++) perm[k] = k;
+        for (const int4& w : work) {
+            std::stable_sort(perm.begin() + w.z, perm.begin() + w.w,
+                             [&](int a, int c) { return b.bcsr_col_id[a] < b.bcsr_col_id[c]; });
+            for (int k = w.z; k < w.w; k++) {
+                col[k] = b.bcsr_col_id[perm[k]];
+                tgt[k] = (unsigned short)(perm[k] - (w.z & ~3));
+            }
         }
+        std::vector<float> data(nd);
+        const size_t al = (size_t)b.bcsr_aligned_size;
+        for (size_t e = 0; e < (size_t)bw * bh; e++) {
+            for (int k = 0; k < nblk; k++) data[e * al + k] = b.bcsr_data[e * al + perm[k]];
+            for (size_t k = nblk; k < al; k++) data[e * al + k] = b.bcsr_data[e * al + k];
+        }
+        if ((rc = upload_int(&p.i1, col.data(), col.size(), col.size())) ||
+            (rc = upload_val(&p.v, data.data(), nd, nd)) ||
+            (rc = alloc(reinterpret_cast<void**>(&p.lcol), tgt.size() * sizeof(unsigned short))) ||
+            (rc = alloc(reinterpret_cast<void**>(&p.blocks), work.size() * sizeof(int4))))
+            return rc;
+        CSP_CUDA(cudaMemcpy(p.lcol, tgt.data(), tgt.size() * sizeof(unsigned short), cudaMemcpyHostToDevice));
+        CSP_CUDA(cudaMemcpy(p.blocks, work.data(), work.size() * sizeof(int4), cudaMemcpyHostToDevice));
+        p.nblocks = (int)work.size();
     }
     parts.push_back(p);
     return CSP_OK;
@@ -805,7 +831,7 @@ static void launch_part(const Part& p, const float* x, float* y, int n, cudaStre
     case PART_GBCSR: {
         if (p.nbr == 0) return;
         if (p.nblocks > 0) {
-#define CSP_GBA(BH, BW) bcsr_adaptive_kernel<V, BH, BW><<<p.nblocks, kGbThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.blocks, p.stride, p.m, n)
+#define CSP_GBA(BH, BW) bcsr_adaptive_kernel<V, BH, BW><<<p.nblocks, kGbThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.blocks, p.lcol, p.stride, p.m, n)
             switch (p.bh * 10 + p.bw) {
             case 11: CSP_GBA(1, 1); break; case 22: CSP_GBA(2, 2); break; case 33: CSP_GBA(3, 3); break;
             case 44: CSP_GBA(4, 4); break;

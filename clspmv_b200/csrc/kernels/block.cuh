@@ -144,12 +144,16 @@ __global__ void __launch_bounds__(256) bcsr_generic_kernel(const int* __restrict
 
 // Generic BCSR, one right-hand side, for blocks of at most 16 elements: the host cuts
 // the block rows into work items {first block row, block rows, first block, end block}
-// of at most kGbBlocks - 3 blocks and kGbRows block rows.  Each thread loads four
-// consecutive blocks -- one 128-bit load of their column ids and one per block element
-// plane, so every matrix byte moves in a coalesced 128-bit load -- and leaves each
-// block's BH row products in shared memory; then a lane group per block row adds its
-// blocks in order (fixed shuffle tree) and updates y.  Requires the block planes'
-// stride (`aligned`) to be a multiple of 4 and the column ids padded to a multiple of 4.
+// of at most kGbBlocks - 3 blocks and kGbRows block rows, and inside each item stores
+// the blocks in column order, with tgt[j] the block's position (relative to the item's
+// first block rounded down to 4) in the row-sorted order.  Each thread loads four
+// consecutive stored blocks -- one 128-bit load of their column ids, one of their
+// targets and one per block element plane, so every matrix byte moves in a coalesced
+// load -- and, since the blocks of a warp are sorted by column, its x gathers touch few
+// cache lines.  Each block's BH row products go to shared memory at its target; then a
+// lane group per block row adds its blocks in row order (fixed shuffle tree) and
+// updates y.  Requires the block planes' stride (`aligned`) to be a multiple of 4 and
+// the column ids and targets padded to a multiple of 4.
 constexpr int kGbThreads = 256;
 constexpr int kGbBlocks = 4 * kGbThreads;
 constexpr int kGbRows = 256;
@@ -183,7 +187,8 @@ template <class V, int BH, int BW>
 __global__ void __launch_bounds__(kGbThreads) bcsr_adaptive_kernel(const int* __restrict__ rp, const int* __restrict__ col,
                                                                    const V* __restrict__ data, const float* __restrict__ x,
                                                                    float* __restrict__ y, const int4* __restrict__ work,
-                                                                   int aligned, int m, int n)
+                                                                   const unsigned short* __restrict__ tgt, int aligned, int m,
+                                                                   int n)
 {
     __shared__ float prod[kGbBlocks * BH];
     __shared__ int s_rp[kGbRows + 1];
@@ -194,9 +199,11 @@ __global__ void __launch_bounds__(kGbThreads) bcsr_adaptive_kernel(const int* __
     const int j = s4 + 4 * tid;
     const bool act = j < e;
     int4 c = make_int4(0, 0, 0, 0);
+    uint2 tg = make_uint2(0, 0);
     float4 d[BH * BW];
     if (act) {
         c = ld_int4(col + j);
+        tg = __ldg(reinterpret_cast<const uint2*>(tgt + j));
 #pragma unroll
         for (int k = 0; k < BH * BW; k++) d[k] = Val<V>::ld4(data + (size_t)k * aligned + j);
     }
@@ -204,6 +211,7 @@ __global__ void __launch_bounds__(kGbThreads) bcsr_adaptive_kernel(const int* __
     if (tid == 0) s_rp[nrows] = e - s4;
     if (act) {
         const int cc[4] = {c.x, c.y, c.z, c.w};
+        const int tq[4] = {(int)(tg.x & 0xffffu), (int)(tg.x >> 16), (int)(tg.y & 0xffffu), (int)(tg.y >> 16)};
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const bool in = j + q >= s && j + q < e;
@@ -219,7 +227,8 @@ __global__ void __launch_bounds__(kGbThreads) bcsr_adaptive_kernel(const int* __
                     const float a = q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w;
                     t += a * xv[w];
                 }
-                prod[(4 * tid + q) * BH + h] = in ? t : 0.0f;
+                // blocks of the previous item (before s) are skipped
+                if (in) prod[tq[q] * BH + h] = t;
             }
         }
     }
