@@ -9,12 +9,14 @@ seeded (the reference's public matrix collection is not available offline).
 One step = one forward SpMV of the whole matrix through the autotuned Cocktail
 engine.  `value` is algorithmic GB/s (values + indices + x + y read/write, no
 padding counted) over the CUDA-event time of the SpMV kernels, inputs resident in
-HBM; L2 (126 MB, larger than this working set) is flushed by a 256 MB write before
-every timed SpMV.  `e2e` is the same metric through the C ABI with host buffers:
+HBM; L2 (126 MB, larger than this working set) is flushed before every timed SpMV by
+a 256 MB write followed by a 256 MB read of another buffer, so neither the workload's
+data nor the flush's own dirty lines (whose write-back would land inside the timed
+region) are left in L2.  `e2e` is the same metric through the C ABI with host buffers:
 H2D of x and y, the SpMV, D2H of y, every step.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload zipf|laplacian|stencil|block]
+                  [--workload zipf|laplacian|stencil|block] [--tune-cache FILE]
 
 With --impl reference the reference's own CPU SpMV (clSpMV_NV/include/spmv_serial.h
 csr_spmv, compiled from the reference sources into oracle/_ref) runs on the same
@@ -204,6 +206,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="zipf", choices=["zipf", "laplacian", "stencil", "block"])
     ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of CPU-baseline sampling")
+    ap.add_argument("--tune-cache", default=None,
+                    help="autotuner decision file: a pattern decided in an earlier run is rebuilt without "
+                         "timing candidates (used to profile the bench's own partition)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -233,7 +238,13 @@ def main():
     # a dedicated stream: the library and torch (flush, events) must launch on the same one
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    flush_w = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    flush_r = torch.ones(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    flush_sink = torch.empty(1, dtype=torch.float32, device="cuda")
+
+    def flush_l2():
+        flush_w.zero_()
+        torch.sum(flush_r, dim=0, out=flush_sink[0])
 
     def time_handle(hd: Handle, steps: int, warmup: int):
         hd.set_stream(stream.cuda_stream)
@@ -241,7 +252,7 @@ def main():
             hd.do_spmv(1)
         evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         for e0, e1 in evs:
-            flush.zero_()
+            flush_l2()
             e0.record(stream)
             hd.do_spmv(1)
             e1.record(stream)
@@ -251,7 +262,7 @@ def main():
     # --- the library's on-device autotuner picks the Cocktail partition ---
     from clspmv_b200 import CSP_ANALYZE_AUTOTUNE, analyze_matrix
     coo = COO(h, w, r, c, v)
-    best_mat = analyze_matrix(coo, mode=CSP_ANALYZE_AUTOTUNE)
+    best_mat = analyze_matrix(coo, mode=CSP_ANALYZE_AUTOTUNE, cache_path=args.tune_cache)
     best_key = best_mat.choice
     best = Handle(best_mat, x, y0)
     # plain single-format CSR on the same GPU: one warp per row (the reference's vector
@@ -307,7 +318,7 @@ def main():
     torch.cuda.synchronize()
     e_times = []
     for _ in range(args.steps):
-        flush.zero_()
+        flush_l2()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         e2e_step()
@@ -344,7 +355,7 @@ def main():
                        "partition": best_key,
                        "plain_csr": {"kernel": plain_key, "gb_s": plain_gbs},
                        "speedup_vs_plain_csr": statistics.median(plain_times) / ms_step,
-                       "l2": "256 MB write between timed SpMVs (working set < L2)",
+                       "l2": "256 MB write then 256 MB read of another buffer between timed SpMVs (working set < L2)",
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": kernel_gbs, "peak": peak, "unit": "GB/s",
                          "frac": kernel_gbs / peak, "peak_source": peak_kind, "traffic": traffic},
