@@ -130,6 +130,14 @@ __global__ void __launch_bounds__(kSpmmThreads) bcsr_spmm4_kernel(const int* __r
         float4 acc[BH];
 #pragma unroll
         for (int h = 0; h < BH; h++) acc[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+        // the Y rows this lane updates, requested before the block loads and X gathers
+        float4 yo[BH];
+#pragma unroll
+        for (int h = 0; h < BH; h++) {
+            const int r = br * BH + h;
+            yo[h] = (valid && active && sub == 0 && r < m) ? *reinterpret_cast<const float4*>(y + (size_t)r * k + c)
+                                                            : make_float4(0.f, 0.f, 0.f, 0.f);
+        }
         for (int j0 = s; j0 < e; j0 += L) {
             const int nb = min(L, e - j0);
             __syncwarp(gmask);
@@ -140,24 +148,36 @@ __global__ void __launch_bounds__(kSpmmThreads) bcsr_spmm4_kernel(const int* __r
             }
             __syncwarp(gmask);
             if (active) {
-                for (int t = sub; t < nb; t += S) {
-                    const int bc = s_col[gbase + t];
-                    const float* bv = s_val + (gbase + t) * BS;
-                    float4 xv[BW];
+                // U blocks of this sub-group at a time: their X rows are requested together
+                constexpr int U = (BW <= 3) ? 4 : 2;
+                for (int t0 = sub; t0 < nb; t0 += S * U) {
+                    float4 xv[U][BW];
 #pragma unroll
-                    for (int w = 0; w < BW; w++)
-                        xv[w] = (bc + w < n) ? __ldg(reinterpret_cast<const float4*>(x + (size_t)(bc + w) * k + c))
-                                             : make_float4(0.f, 0.f, 0.f, 0.f);
+                    for (int u = 0; u < U; u++) {
+                        const int t = t0 + u * S;
+                        const int bc = t < nb ? s_col[gbase + t] : 0;
 #pragma unroll
-                    for (int h = 0; h < BH; h++)
+                        for (int w = 0; w < BW; w++)
+                            xv[u][w] = (t < nb && bc + w < n)
+                                           ? __ldg(reinterpret_cast<const float4*>(x + (size_t)(bc + w) * k + c))
+                                           : make_float4(0.f, 0.f, 0.f, 0.f);
+                    }
 #pragma unroll
-                        for (int w = 0; w < BW; w++) {
-                            const float a = bv[h * BW + w];
-                            acc[h].x += a * xv[w].x;
-                            acc[h].y += a * xv[w].y;
-                            acc[h].z += a * xv[w].z;
-                            acc[h].w += a * xv[w].w;
-                        }
+                    for (int u = 0; u < U; u++) {
+                        const int t = t0 + u * S;
+                        if (t >= nb) break;
+                        const float* bv = s_val + (gbase + t) * BS;
+#pragma unroll
+                        for (int h = 0; h < BH; h++)
+#pragma unroll
+                            for (int w = 0; w < BW; w++) {
+                                const float a = bv[h * BW + w];
+                                acc[h].x += a * xv[u][w].x;
+                                acc[h].y += a * xv[u][w].y;
+                                acc[h].z += a * xv[u][w].z;
+                                acc[h].w += a * xv[u][w].w;
+                            }
+                    }
                 }
             }
         }
@@ -177,13 +197,12 @@ __global__ void __launch_bounds__(kSpmmThreads) bcsr_spmm4_kernel(const int* __r
             for (int h = 0; h < BH; h++) {
                 const int r = br * BH + h;
                 if (r < m) {
-                    float4* yp = reinterpret_cast<float4*>(y + (size_t)r * k + c);
-                    float4 o = *yp;
+                    float4 o = yo[h];
                     o.x += acc[h].x;
                     o.y += acc[h].y;
                     o.z += acc[h].z;
                     o.w += acc[h].w;
-                    *yp = o;
+                    *reinterpret_cast<float4*>(y + (size_t)r * k + c) = o;
                 }
             }
         }
