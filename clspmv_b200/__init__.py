@@ -23,10 +23,12 @@ import numpy as np
 
 from . import capi
 from .capi import (COO, CSP_ANALYZE_AUTOTUNE, CSP_ANALYZE_REFERENCE, CSP_FLAG_ADJOINT, CSP_FLAG_BF16,
+                   CSP_FLAG_L2_PERSIST, CSP_METH_XPANEL,
                    CSP_FLAG_GRAPH, CSP_FLAG_USE_TEX, CspError, check, lib, to_numpy)
 
 __all__ = ["COO", "Cocktail", "Handle", "analyze_matrix", "init_mat_kernels", "spmv_all", "evaluate",
            "CspError", "CSP_FLAG_BF16", "CSP_FLAG_GRAPH", "CSP_FLAG_USE_TEX", "CSP_FLAG_ADJOINT",
+           "CSP_FLAG_L2_PERSIST", "CSP_METH_XPANEL",
            "CSP_ANALYZE_REFERENCE", "CSP_ANALYZE_AUTOTUNE", "lib", "Batch"]
 
 from .batch import Batch  # noqa: E402
@@ -146,6 +148,10 @@ class Handle:
 
     def do_spmv(self, ntimes: int = 1):
         check(lib().csp_do_spmv(self.h, int(ntimes)), "do_spmv")
+
+    def iterate(self, iterations: int):
+        """eval.cpp:19 example() on the device: `iterations` times res += A*vec; vec = res."""
+        check(lib().csp_iterate(self.h, int(iterations)), "iterate")
 
     def synchronize(self):
         check(lib().csp_synchronize(self.h), "synchronize")

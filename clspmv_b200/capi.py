@@ -19,7 +19,8 @@ IP = C.POINTER(C.c_int)
 FP = C.POINTER(C.c_float)
 
 CSP_OK, CSP_EINVAL, CSP_ENOMEM, CSP_ECUDA, CSP_EFORMAT, CSP_ENODEV, CSP_EUNSUP, CSP_EIO, CSP_ETIMEOUT = range(9)
-CSP_FLAG_USE_TEX, CSP_FLAG_BF16, CSP_FLAG_GRAPH, CSP_FLAG_ADJOINT = 0x1, 0x2, 0x4, 0x8
+CSP_FLAG_USE_TEX, CSP_FLAG_BF16, CSP_FLAG_GRAPH, CSP_FLAG_ADJOINT, CSP_FLAG_L2_PERSIST = 0x1, 0x2, 0x4, 0x8, 0x10
+CSP_METH_XPANEL = 16
 CSP_ANALYZE_REFERENCE, CSP_ANALYZE_AUTOTUNE = 0, 1
 CSP_NOALLOC_MAX_NNZ = 33554432
 CSP_BFMT_AUTO = -1
@@ -199,6 +200,7 @@ def _declare(lib):
         "csp_analyze_matrix": (C.c_int, [P(coo_matrix), P(cocktail), P(csp_analyze_opts)]),
         "csp_init_mat_kernels": (C.c_int, [P(cocktail), FP, FP, C.c_int, P(C.c_void_p)]),
         "csp_do_spmv": (C.c_int, [C.c_void_p, C.c_int]),
+        "csp_iterate": (C.c_int, [C.c_void_p, C.c_int]),
         "csp_init_mat_kernels_ex": (C.c_int, [P(cocktail), FP, FP, C.c_int, C.c_int, P(C.c_void_p)]),
         "csp_init_bcsr_kernels": (C.c_int, [P(bcsr_matrix), FP, FP, C.c_int, C.c_int, P(C.c_void_p)]),
         "csp_synchronize": (C.c_int, [C.c_void_p]),

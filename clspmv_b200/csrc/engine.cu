@@ -105,6 +105,14 @@ int Engine::upload_val(void** d, const float* h, size_t n, size_t cap)
 Engine::~Engine()
 {
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    for (auto& kv : iter_graphs) if (kv.second) cudaGraphExecDestroy(kv.second);
+    if (l2_window && own_stream) {
+        // drop the window and return the persisting lines to normal use
+        cudaStreamAttrValue attr = {};
+        attr.accessPolicyWindow.num_bytes = 0;
+        cudaStreamSetAttribute(own_stream, cudaStreamAttributeAccessPolicyWindow, &attr);
+        cudaCtxResetPersistingL2Cache();
+    }
     for (void* p : allocations) cudaFree(p);
     if (own_stream) cudaStreamDestroy(own_stream);
 }
@@ -903,6 +911,95 @@ int Engine::spmv(int ntimes)
     return CSP_OK;
 }
 
+// The reference's solver loop (eval.cpp:19 example(): do_spmv, then the result becomes
+// the next vector) on the device: `iterations` times y += A x; x = y.  With
+// CSP_FLAG_GRAPH, kIterChunk iterations are captured as one CUDA graph (and the
+// remainder as another), so a long loop costs one graph launch per chunk.
+int Engine::iterate_once(cudaStream_t st)
+{
+    int rc = enqueue_once(st);
+    if (rc) return rc;
+    CSP_CUDA(cudaMemcpyAsync(d_x, d_y, (size_t)height * sizeof(float), cudaMemcpyDeviceToDevice, st));
+    return CSP_OK;
+}
+
+int Engine::iterate(int iterations)
+{
+    if (iterations < 0) return set_error(CSP_EINVAL, "iterations < 0");
+    if (width != height) return set_error(CSP_EINVAL, "iterate needs a square matrix (%d x %d)", height, width);
+    if (nrhs != 1) return set_error(CSP_EUNSUP, "iterate with several right-hand sides");
+    cudaStream_t st = stream;
+    if (!use_graph) {
+        for (int i = 0; i < iterations; i++) {
+            int rc = iterate_once(st);
+            if (rc) return rc;
+        }
+        return CSP_OK;
+    }
+    auto graph_of = [&](int n, cudaGraphExec_t* out) -> int {
+        cudaGraphExec_t& ge = iter_graphs[n];
+        if (!ge || iter_stream != st) {
+            if (ge) { cudaGraphExecDestroy(ge); ge = nullptr; }
+            cudaGraph_t g;
+            CSP_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+            int rc = CSP_OK;
+            for (int i = 0; i < n && !rc; i++) rc = iterate_once(st);
+            cudaError_t e = cudaStreamEndCapture(st, &g);
+            if (rc) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
+            if (e != cudaSuccess) return cuda_error(e, "cudaStreamEndCapture");
+            e = cudaGraphInstantiate(&ge, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_error(e, "cudaGraphInstantiate");
+        }
+        *out = ge;
+        return CSP_OK;
+    };
+    if (iter_stream != st) {
+        for (auto& kv : iter_graphs) if (kv.second) cudaGraphExecDestroy(kv.second);
+        iter_graphs.clear();
+    }
+    int rc;
+    cudaGraphExec_t ge = nullptr;
+    const int full = iterations / kIterChunk, rest = iterations % kIterChunk;
+    if (full) {
+        if ((rc = graph_of(kIterChunk, &ge))) return rc;
+        for (int i = 0; i < full; i++) CSP_CUDA(cudaGraphLaunch(ge, st));
+    }
+    if (rest) {
+        if ((rc = graph_of(rest, &ge))) return rc;
+        CSP_CUDA(cudaGraphLaunch(ge, st));
+    }
+    iter_stream = st;
+    return CSP_OK;
+}
+
+// CSP_FLAG_L2_PERSIST: x (all right-hand sides) marked persisting in L2 for the
+// handle's own stream, with as much persisting L2 reserved for this process's context
+// as the device allows (up to the size of x).  The reservation and the window end with
+// the context / the handle.
+int Engine::set_l2_window()
+{
+    int dev_id = 0, max_persist = 0, max_window = 0;
+    CSP_CUDA(cudaGetDevice(&dev_id));
+    CSP_CUDA(cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev_id));
+    CSP_CUDA(cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev_id));
+    if (max_persist <= 0 || max_window <= 0) return set_error(CSP_EUNSUP, "device has no persisting L2");
+    const size_t xb = (size_t)x_len * nrhs * sizeof(float);
+    size_t cur = 0;
+    CSP_CUDA(cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize));
+    const size_t want = std::min(xb, (size_t)max_persist);
+    if (cur < want) CSP_CUDA(cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want));
+    cudaStreamAttrValue attr = {};
+    attr.accessPolicyWindow.base_ptr = d_x;
+    attr.accessPolicyWindow.num_bytes = std::min(xb, (size_t)max_window);
+    attr.accessPolicyWindow.hitRatio = std::min(1.0f, (float)want / (float)attr.accessPolicyWindow.num_bytes);
+    attr.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+    attr.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+    CSP_CUDA(cudaStreamSetAttribute(own_stream, cudaStreamAttributeAccessPolicyWindow, &attr));
+    l2_window = true;
+    return CSP_OK;
+}
+
 int Engine::init_common(int w, int h, int nz, const float* vec, const float* res, int flags, int k)
 {
     width = w;
@@ -930,6 +1027,7 @@ int Engine::init_common(int w, int h, int nz, const float* vec, const float* res
     CSP_CUDA(cudaMemset(d_y, 0, (size_t)y_len * nrhs * 4));
     if (vec && width) CSP_CUDA(cudaMemcpy(d_x, vec, (size_t)width * nrhs * 4, cudaMemcpyHostToDevice));
     if (res && height) CSP_CUDA(cudaMemcpy(d_y, res, (size_t)height * nrhs * 4, cudaMemcpyHostToDevice));
+    if ((flags & CSP_FLAG_L2_PERSIST) && (rc = set_l2_window())) return rc;
     return CSP_OK;
 }
 
@@ -1035,6 +1133,7 @@ int csp_init_bcsr_kernels(const bcsr_matrix_if* b, const float* vec, const float
 }
 
 int csp_do_spmv(csp_handle* h, int ntimes) { CSP_HANDLE_CHECK(h); return h->eng.spmv(ntimes); }
+int csp_iterate(csp_handle* h, int iterations) { CSP_HANDLE_CHECK(h); return h->eng.iterate(iterations); }
 
 int csp_synchronize(csp_handle* h)
 {

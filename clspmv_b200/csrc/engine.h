@@ -5,6 +5,7 @@
 #include <stddef.h>
 #include <stdint.h>
 #include <string.h>
+#include <map>
 #include <vector>
 
 #include "csp/clspmv.h"
@@ -75,6 +76,10 @@ struct Engine {
     size_t device_bytes = 0;
     cudaGraphExec_t graph_exec = nullptr;
     cudaStream_t graph_stream = nullptr;
+    std::map<int, cudaGraphExec_t> iter_graphs;   // csp_iterate: graphs of n iterations
+    cudaStream_t iter_stream = nullptr;
+    bool l2_window = false;                         // CSP_FLAG_L2_PERSIST applied to own_stream
+    static constexpr int kIterChunk = 32;
     // adjoint (CSP_FLAG_ADJOINT)
     bool adjoint = false;
     bool abar_blocks = false;          // a block-format part: no value gradients
@@ -87,6 +92,9 @@ struct Engine {
     int init_common(int w, int h, int nz, const float* vec, const float* res, int flags, int k);
     int init_bcsr(const bcsr_matrix_if* b, const float* vec, const float* res, int flags, int k);
     int spmv(int ntimes);
+    int iterate(int iterations);
+    int iterate_once(cudaStream_t st);
+    int set_l2_window();
     int enqueue_once(cudaStream_t st);
     int enqueue_parts(const std::vector<Part>& ps, const float* x, float* y, int n, cudaStream_t st);
     int build_adjoint(const cocktail_iif* mat);

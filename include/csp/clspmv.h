@@ -310,6 +310,10 @@ typedef struct csp_handle csp_handle;
 #define CSP_FLAG_BF16      0x2  /* store matrix values as BF16, accumulate in FP32                             */
 #define CSP_FLAG_GRAPH     0x4  /* replay do_spmv as one captured CUDA graph                                   */
 #define CSP_FLAG_ADJOINT   0x8  /* also build the transposed structures for csp_spmv_adjoint                  */
+#define CSP_FLAG_L2_PERSIST 0x10 /* keep x resident in L2: an access-policy window (persisting hits) over x on
+                                    the handle's own stream, with persisting L2 reserved for this process's
+                                    context up to x's size; not applied to a stream given by csp_set_stream.
+                                    No counterpart in the reference. */
 
 /* Kernel choice for a CSR or COO sub-matrix (csr_meth_num / coo_meth_num; no
  * counterpart in the reference): x staged in shared memory by column panels of at
@@ -338,6 +342,11 @@ int csp_init_bcsr_kernels(const bcsr_matrix_if* mat, const float* vec, const flo
                           csp_handle** out);
 /* Enqueue ntimes SpMVs res += A*vec on the handle's stream.  (:1091 do_spmv) */
 int csp_do_spmv(csp_handle* h, int ntimes);
+/* The solver loop of the reference's example() (eval.cpp:19-50: do_spmv, then
+ * cpy_vector_from_gpu(gpumat.res)) on the device: `iterations` times res += A*vec
+ * followed by vec = res.  Square matrices, one right-hand side.  With CSP_FLAG_GRAPH
+ * every 32 iterations are one CUDA graph launch.  Asynchronous on the handle's stream. */
+int csp_iterate(csp_handle* h, int iterations);
 /* Block until every launch on the handle's stream has finished. */
 int csp_synchronize(csp_handle* h);
 int csp_cpy_vector_from_cpu(csp_handle* h, const float* vec, int vec_size);     /* :1462 */
