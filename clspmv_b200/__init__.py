@@ -28,7 +28,7 @@ from .capi import (COO, CSP_ANALYZE_AUTOTUNE, CSP_ANALYZE_REFERENCE, CSP_FLAG_AD
 
 __all__ = ["COO", "Cocktail", "Handle", "analyze_matrix", "init_mat_kernels", "spmv_all", "evaluate",
            "CspError", "CSP_FLAG_BF16", "CSP_FLAG_GRAPH", "CSP_FLAG_USE_TEX", "CSP_FLAG_ADJOINT",
-           "CSP_FLAG_L2_PERSIST", "CSP_METH_XPANEL",
+           "CSP_FLAG_L2_PERSIST", "CSP_METH_XPANEL", "benchmark_tables",
            "CSP_ANALYZE_REFERENCE", "CSP_ANALYZE_AUTOTUNE", "lib", "Batch"]
 
 from .batch import Batch  # noqa: E402
@@ -237,6 +237,13 @@ class Handle:
             self.free()
         except Exception:
             pass
+
+
+def benchmark_tables(clspmv_path: str, level: int = 1) -> None:
+    """Write the analyzer's calibration tables, measured on this GPU, under
+    clspmv_path/benchmark (the reference's bench_* programs; csp_benchmark_tables).
+    analyze_matrix(coo, bench_path=clspmv_path) then partitions from them."""
+    check(lib().csp_benchmark_tables(clspmv_path.encode(), int(level)), "benchmark_tables")
 
 
 def init_mat_kernels(mat: Cocktail, vec=None, res=None, flags: int = 0) -> Handle:

@@ -201,6 +201,7 @@ def _declare(lib):
         "csp_init_mat_kernels": (C.c_int, [P(cocktail), FP, FP, C.c_int, P(C.c_void_p)]),
         "csp_do_spmv": (C.c_int, [C.c_void_p, C.c_int]),
         "csp_iterate": (C.c_int, [C.c_void_p, C.c_int]),
+        "csp_benchmark_tables": (C.c_int, [C.c_char_p, C.c_int]),
         "csp_init_mat_kernels_ex": (C.c_int, [P(cocktail), FP, FP, C.c_int, C.c_int, P(C.c_void_p)]),
         "csp_init_bcsr_kernels": (C.c_int, [P(bcsr_matrix), FP, FP, C.c_int, C.c_int, P(C.c_void_p)]),
         "csp_synchronize": (C.c_int, [C.c_void_p]),

@@ -297,6 +297,16 @@ typedef struct csp_analyze_opts {
  * fastest, and records the choice under a hash of the sparsity pattern in
  * cache_path (if given) so the next call on the same pattern skips timing. */
 int csp_analyze_matrix(coo_matrix_if* coo, cocktail_iif* mat, const csp_analyze_opts* opts);
+/* Measure this library's kernels on the current GPU and write the analyzer's
+ * calibration tables (clspmv_path/benchmark/{overhead,dia,bdia,ell,sell,csr,coo,bcsr,
+ * bell,sbell}.ben) in the layout the reference's bench_* programs write
+ * (clSpMV_NV/src/bench_*.cpp, the `benchmarking` script): the same synthetic banded
+ * matrices, one GFLOPS column per kernel method.  CSP_ANALYZE_REFERENCE with
+ * bench_path = clspmv_path then partitions from B200 measurements.  level 2: the
+ * reference's full grids (minutes); 1: every third size and every other width;
+ * 0: two sizes and two widths per table (seconds; a format check).  Synchronous. */
+int csp_benchmark_tables(const char* clspmv_path, int level);
+
 /* Name of the partition the last AUTOTUNE call on this thread chose ("" if none),
  * e.g. "csr2", "ell1+csr2", "bcsr4x4m0". */
 const char* csp_autotune_choice(void);
