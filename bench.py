@@ -68,27 +68,28 @@ def _peak():
 WORKLOADS = ["zipf", "laplacian", "stencil", "block", "batch"]
 
 
-def make_workload(name: str):
+def make_workload(name: str, scale: float = 1.0):
     """(description, list of matrices (h, w, row, col, val), x, y0); for the batch the
-    vectors are the matrices' vectors concatenated in order."""
+    vectors are the matrices' vectors concatenated in order.  scale < 1 shrinks the
+    workload (rows, grid edge, block rows or matrix count) for profiling runs."""
     from clspmv_b200 import matrices as M
     if name == "batch":
-        mats = [m[1:] for m in M.batch_mixed()]
+        mats = [m[1:] for m in M.batch_mixed(max(1, int(round(512 * scale))))]
         W = sum(m[1] for m in mats)
         H = sum(m[0] for m in mats)
         return ("batch_mixed 512 matrices, rows log-uniform in [1,000, 200,000], Laplacian / Zipf / 3x3-block, FP32",
                 mats, M.vector(W, seed=1), M.vector(H, seed=2))
     if name == "zipf":
-        case = M.zipf_rows(1_000_000, 2.0, 10_000, seed=0)
+        case = M.zipf_rows(max(1000, int(1_000_000 * scale)), 2.0, 10_000, seed=0)
         desc = "zipf_rows n=1,000,000 s=2.0 len<=10,000 FP32"
     elif name == "laplacian":
-        case = M.laplacian_2d(128)
+        case = M.laplacian_2d(max(8, int(round(128 * scale ** 0.5))))
         desc = "laplacian_2d 128x128 (16,384 rows) FP32"
     elif name == "stencil":
-        case = M.stencil_27(160)
+        case = M.stencil_27(max(8, int(round(160 * scale ** (1.0 / 3.0)))))
         desc = "stencil_27 160^3 (4,096,000 rows) FP32"
     elif name == "block":
-        case = M.block_3x3(500_000)
+        case = M.block_3x3(max(1000, int(500_000 * scale)))
         desc = "block_3x3 500,000 block rows (3x3 blocks, block-row degree U[10,30], band +-2000) FP32"
     else:
         raise ValueError(name)
@@ -249,6 +250,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="zipf", choices=WORKLOADS)
     ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of CPU-baseline sampling")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="shrink the workload (profiling runs only; the benchmark configuration is 1.0)")
     ap.add_argument("--tune-cache", default=None,
                     help="autotuner decision file: a pattern decided in an earlier run is rebuilt without "
                          "timing candidates (used to profile the bench's own partition)")
@@ -262,7 +265,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        desc, mats, x, y0 = make_workload(args.workload)
+        desc, mats, x, y0 = make_workload(args.workload, args.scale)
         run_reference_arm(args, desc, mats, x, y0)
         return
 
@@ -276,7 +279,9 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
 
     wl = args.workload
-    desc, mats, x, y0 = make_workload(wl)
+    desc, mats, x, y0 = make_workload(wl, args.scale)
+    if args.scale != 1.0:
+        desc += f" (scaled x{args.scale:g} for profiling)"
     nnz = int(sum(m[2].size for m in mats))
     ab = workload_bytes(wl, mats)
     # a dedicated stream: the library and torch (flush, events) must launch on the same one
