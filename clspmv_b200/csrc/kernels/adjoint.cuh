@@ -39,11 +39,12 @@ __global__ void __launch_bounds__(256) abar_dia_kernel(const int* __restrict__ o
 }
 
 // Value gradients of DIA-layout slots, four rows per thread over every diagonal: the
-// thread's ybar values are loaded once, x is read around row r + off[d] (neighbouring
-// threads share those lines in L1), and each diagonal gets one 128-bit streaming store,
-// so a warp writes 512 contiguous bytes per diagonal.  No 64-bit index division.
-// len is a multiple of 4 and abar is 16-byte aligned (checked by the host); the
-// offsets (nd of them) are staged in shared memory.
+// thread's ybar values are loaded once, x around row r + off[d] comes from two aligned
+// 128-bit loads (scalar, guarded loads at the matrix edges), and each diagonal gets one
+// 128-bit streaming store, so a warp writes 512 contiguous bytes per diagonal.  No
+// 64-bit index division.  len is a multiple of 4, abar is 16-byte aligned (checked by
+// the host) and x is the handle's padded x; the offsets (nd of them) are staged in
+// shared memory.
 __global__ void __launch_bounds__(256) abar_dia4_kernel(const int* __restrict__ off, int nd, int len, int m, int n,
                                                         const float* __restrict__ ybar, const float* __restrict__ x,
                                                         float* __restrict__ abar)
@@ -57,14 +58,25 @@ __global__ void __launch_bounds__(256) abar_dia4_kernel(const int* __restrict__ 
 #pragma unroll
     for (int q = 0; q < 4; q++) yb[q] = r + q < m ? __ldg(ybar + r + q) : 0.0f;
     for (int d = 0; d < nd; d++) {
-        const int o = s_off[d];
-        float g[4];
+        const int base = r + s_off[d];
+        float xv[4];
+        if (base >= 0 && base + 3 < n) {
+            // x[base .. base+3] from the two aligned float4s around it (x is 16-byte
+            // aligned and zero-padded by at least 64 entries past n)
+            const int b4 = base & ~3;
+            const float4 lo = ldx4(x, b4), hi = ldx4(x, b4 + 4);
+            switch (base - b4) {
+            case 0: xv[0] = lo.x; xv[1] = lo.y; xv[2] = lo.z; xv[3] = lo.w; break;
+            case 1: xv[0] = lo.y; xv[1] = lo.z; xv[2] = lo.w; xv[3] = hi.x; break;
+            case 2: xv[0] = lo.z; xv[1] = lo.w; xv[2] = hi.x; xv[3] = hi.y; break;
+            default: xv[0] = lo.w; xv[1] = hi.x; xv[2] = hi.y; xv[3] = hi.z; break;
+            }
+        } else {
 #pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int c = r + q + o;
-            g[q] = (c >= 0 && c < n) ? yb[q] * __ldg(x + c) : 0.0f;
+            for (int q = 0; q < 4; q++) xv[q] = (base + q >= 0 && base + q < n) ? __ldg(x + base + q) : 0.0f;
         }
-        __stcs(reinterpret_cast<float4*>(abar + (size_t)d * len + r), make_float4(g[0], g[1], g[2], g[3]));
+        __stcs(reinterpret_cast<float4*>(abar + (size_t)d * len + r),
+               make_float4(yb[0] * xv[0], yb[1] * xv[1], yb[2] * xv[2], yb[3] * xv[3]));
     }
 }
 
