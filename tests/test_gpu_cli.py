@@ -53,3 +53,12 @@ def test_spmv_cocktail_cli(tmp_path, tables):
     assert out.returncode == 0, out.stderr
     assert "Partition (" + ("reference tables" if tables else "autotuned") in out.stdout
     assert "GFLOPS" in out.stdout
+
+
+def test_gather_rates_are_positive():
+    """csp_gather_test: the L2, shared-memory and cluster gather probes run and report
+    rates (cluster -1 only where the device has no thread-block clusters)."""
+    from clspmv_b200 import gather_test
+    r = gather_test()
+    assert r["l2_per_s"] > 0 and r["shared_per_s"] > 0
+    assert r["cluster_per_s"] > 0 or r["cluster_per_s"] == -1.0
