@@ -15,6 +15,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <algorithm>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -294,18 +295,12 @@ std::vector<std::string> candidates(const Coo& a)
         }
     }
     if (h == w && nnz > 0) {
-        // DIA only if the padded storage stays within the reference's 2x rule; probed by conversion
-        dia_matrix_iif d;
-        csp_init_dia_matrix(&d);
-        coo_matrix_if* mm = const_cast<coo_matrix_if*>(m);
-        if (csp_coo2dia(mm, &d, 32) == CSP_OK) {
-            c.push_back("dia0");
-            c.push_back("dia1");
-            c.push_back("bdia0");
-            c.push_back("bdia1");
-        }
-        csp_free_dia_matrix(&d);
-        clear_error();
+        // DIA only if the padded storage stays within the reference's 2x rule: a failed
+        // conversion drops the DIA and BDIA candidates (see autotune_partition)
+        c.push_back("dia0");
+        c.push_back("dia1");
+        c.push_back("bdia0");
+        c.push_back("bdia1");
     }
     static const int bhs[4] = {1, 2, 4, 8};
     for (int bw : {4, 8})
@@ -352,6 +347,27 @@ int time_candidate(const cocktail_iif* c, int flags, void* flush, size_t flush_b
     std::sort(t.begin(), t.end());
     *ms = t[t.size() / 2];
     return CSP_OK;
+}
+
+// Candidates that differ only in the kernel method share one conversion: the key of
+// that conversion ("" for candidates converted on their own), and the method applied to
+// a shared copy.
+std::string conversion_key(const std::string& name)
+{
+    int x = 0, y = 0, z = 0;
+    if (name.find('+') != std::string::npos) return "";
+    if (sscanf(name.c_str(), "bcsr%dx%dm%d", &x, &y, &z) == 3) return "bcsr" + std::to_string(x) + "x" + std::to_string(y);
+    if (sscanf(name.c_str(), "bdia%d", &x) == 1) return "bdia";
+    if (sscanf(name.c_str(), "dia%d", &x) == 1) return "dia";
+    return "";
+}
+
+void set_method(const std::string& name, cocktail_iif* c)
+{
+    int x = 0, y = 0, z = 0;
+    if (sscanf(name.c_str(), "bcsr%dx%dm%d", &x, &y, &z) == 3) c->bcsr_meth_num = z;
+    else if (sscanf(name.c_str(), "bdia%d", &x) == 1) c->bdia_meth_num = x;
+    else if (sscanf(name.c_str(), "dia%d", &x) == 1) c->dia_meth_num = x;
 }
 
 bool cache_lookup(const char* path, uint64_t key, std::string& name)
@@ -409,22 +425,48 @@ int autotune_partition(coo_matrix_if* coo, cocktail_iif* out, const csp_analyze_
     void* flush = nullptr;
     if (cudaMalloc(&flush, flush_bytes) != cudaSuccess) return set_error(CSP_ENOMEM, "autotune flush buffer");
     double best_ms = 1e30;
+    // conversions shared by several candidates, owned here until the end; `best_conv` is
+    // the key of the one the best candidate shares ("" if it owns its arrays)
+    std::map<std::string, cocktail_iif> conv;
+    std::map<std::string, bool> conv_failed;
+    std::string best_conv;
     for (const std::string& name : candidates(a)) {
+        const std::string key = conversion_key(name);
         cocktail_iif c;
-        if (build(a, name, &c) != CSP_OK) { csp_free_cocktail(&c); clear_error(); continue; }
+        if (key.empty()) {
+            if (build(a, name, &c) != CSP_OK) { csp_free_cocktail(&c); clear_error(); continue; }
+        } else {
+            if (conv_failed[key]) continue;
+            auto it = conv.find(key);
+            if (it == conv.end()) {
+                cocktail_iif cc;
+                if (build(a, name, &cc) != CSP_OK) {
+                    csp_free_cocktail(&cc);
+                    clear_error();
+                    conv_failed[key] = true;
+                    continue;
+                }
+                it = conv.emplace(key, cc).first;
+            }
+            c = it->second;   // shallow: the arrays stay owned by conv
+            set_method(name, &c);
+        }
         double ms = 0.0;
         const int trc = time_candidate(&c, flags, flush, flush_bytes, 5, &ms);
         if (opts->verbose) printf("autotune %-16s %s %.3f us\n", name.c_str(), trc ? "failed" : "", ms * 1e3);
         if (trc == CSP_OK && ms < best_ms) {
-            if (!best.empty()) csp_free_cocktail(out);
+            if (!best.empty() && best_conv.empty()) csp_free_cocktail(out);
             *out = c;
             best = name;
             best_ms = ms;
+            best_conv = key;
         } else {
-            csp_free_cocktail(&c);
+            if (key.empty()) csp_free_cocktail(&c);
             clear_error();
         }
     }
+    for (auto& kv : conv)
+        if (kv.first != best_conv) csp_free_cocktail(&kv.second);
     cudaFree(flush);
     if (best.empty()) return set_error(CSP_EFORMAT, "autotune: no candidate partition ran");
     g_choice = best;
