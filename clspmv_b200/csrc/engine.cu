@@ -604,7 +604,7 @@ int Engine::add_generic_bcsr(const bcsr_matrix_if& b, int method)
     p.m = b.matinfo.height;
     p.nbr = b.bcsr_row_num;
     p.stride = b.bcsr_aligned_size;
-    const size_t nd = (size_t)b.bcsr_aligned_size * bw * bh;
+    size_t nd = (size_t)b.bcsr_aligned_size * bw * bh;
     int rc;
     if ((rc = check_row_ptr(b.bcsr_row_ptr, b.bcsr_row_num, "generic BCSR"))) return rc;
     if (b.bcsr_row_ptr[b.bcsr_row_num] > b.bcsr_block_num) return set_error(CSP_EINVAL, "generic BCSR: row pointer past the blocks");
@@ -612,9 +612,9 @@ int Engine::add_generic_bcsr(const bcsr_matrix_if& b, int method)
     if ((rc = upload_int(&p.i0, b.bcsr_row_ptr, (size_t)b.bcsr_row_num + 1, (size_t)b.bcsr_row_num + 1))) return rc;
     // one right-hand side, blocks of at most 16 elements: work items of whole block rows
     // for the adaptive kernel (kernels/block.cuh bcsr_adaptive_kernel), unless a block
-    // row is too long for one CTA or the planes' stride is not a multiple of 4
+    // row is too long for one CTA
     std::vector<int4> work;
-    bool fits = nrhs == 1 && bw * bh <= 16 && b.bcsr_aligned_size % 4 == 0;
+    bool fits = nrhs == 1 && bw * bh <= 16;
     if (fits) {
         const int* rp = b.bcsr_row_ptr;
         int r0 = 0;
@@ -634,24 +634,38 @@ int Engine::add_generic_bcsr(const bcsr_matrix_if& b, int method)
             (rc = upload_val(&p.v, b.bcsr_data, nd, nd)))
             return rc;
     } else {
-        // inside each item, blocks in column order (stable); tgt = row-order position - (s & ~3)
-        std::vector<int> perm((size_t)nblk), col((size_t)pad_to(nblk, 4) + 4, 0);
-        std::vector<unsigned short> tgt(col.size(), 0);
+        // each item at a multiple of 4, its blocks in column order (stable) dealt to the
+        // lanes of its 128-block chunks (kernels/block.cuh); tgt = row-order position - s,
+        // 0xffff on empty slots
+        std::vector<int> perm((size_t)nblk);
         for (int k = 0; k < nblk; k++) perm[k] = k;
-        for (const int4& w : work) {
-            std::stable_sort(perm.begin() + w.z, perm.begin() + w.w,
+        size_t total = 0;
+        for (const int4& w : work) total += (size_t)pad_to(w.w - w.z, 4);
+        std::vector<int> col(total + 4, 0), src(total, -1);
+        std::vector<unsigned short> tgt(col.size(), 0xffff);
+        size_t ds = 0;
+        for (int4& w : work) {
+            const int s = w.z, cnt = w.w - w.z;
+            std::stable_sort(perm.begin() + s, perm.begin() + w.w,
                              [&](int a, int c) { return b.bcsr_col_id[a] < b.bcsr_col_id[c]; });
-            for (int k = w.z; k < w.w; k++) {
-                col[k] = b.bcsr_col_id[perm[k]];
-                tgt[k] = (unsigned short)(perm[k] - (w.z & ~3));
+            const int nfull = cnt / 128, tail_lanes = pad_to(cnt - 128 * nfull, 4) / 4;
+            for (int rk = 0; rk < cnt; rk++) {
+                const int base = rk / 128 * 128, T = rk / 128 < nfull ? 32 : tail_lanes, r = rk - base;
+                const size_t slot = ds + (size_t)(base + 4 * (r % T) + r / T);
+                src[slot] = perm[s + rk];
+                col[slot] = b.bcsr_col_id[perm[s + rk]];
+                tgt[slot] = (unsigned short)(perm[s + rk] - s);
             }
+            w.y |= cnt << 16;
+            w.w = (int)ds;
+            ds += (size_t)pad_to(cnt, 4);
         }
+        p.stride = (int)total;
+        nd = total * bw * bh;
         std::vector<float> data(nd);
         const size_t al = (size_t)b.bcsr_aligned_size;
-        for (size_t e = 0; e < (size_t)bw * bh; e++) {
-            for (int k = 0; k < nblk; k++) data[e * al + k] = b.bcsr_data[e * al + perm[k]];
-            for (size_t k = nblk; k < al; k++) data[e * al + k] = b.bcsr_data[e * al + k];
-        }
+        for (size_t e = 0; e < (size_t)bw * bh; e++)
+            for (size_t k = 0; k < total; k++) data[e * total + k] = src[k] < 0 ? 0.0f : b.bcsr_data[e * al + src[k]];
         if ((rc = upload_int(&p.i1, col.data(), col.size(), col.size())) ||
             (rc = upload_val(&p.v, data.data(), nd, nd)) ||
             (rc = alloc(reinterpret_cast<void**>(&p.lcol), tgt.size() * sizeof(unsigned short))) ||

@@ -142,24 +142,29 @@ __global__ void __launch_bounds__(256) bcsr_generic_kernel(const int* __restrict
     }
 }
 
-// Generic BCSR, one right-hand side, for blocks of at most 16 elements: the host cuts
-// the block rows into work items {first block row, block rows, first block, end block}
-// of at most kGbBlocks - 3 blocks and kGbRows block rows, and inside each item stores
-// the blocks in column order, with tgt[j] the block's position (relative to the item's
-// first block rounded down to 4) in the row-sorted order.  Each thread loads four
-// consecutive stored blocks -- one 128-bit load of their column ids, one of their
-// targets and one per block element plane, so every matrix byte moves in a coalesced
-// load -- and, since the blocks of a warp are sorted by column, its x gathers touch few
-// cache lines.  Each block's BH row products go to shared memory at its target; then a
-// lane group per block row adds its blocks in row order (fixed shuffle tree) and
-// updates y.  Requires the block planes' stride (`aligned`) to be a multiple of 4 and
-// the column ids and targets padded to a multiple of 4.
+// Generic BCSR, one right-hand side, for blocks of at most 16 elements.  The host cuts
+// the block rows into work items of at most kGbBlocks - 3 blocks and kGbRows block rows
+// and lays each item out on its own: its blocks start at a multiple of 4 (`ds`) and are
+// in column order (stable), dealt to lanes so that lane t of warp w holds the column
+// ranks 128w + qT + t (q < 4; T = 32, or a quarter of the item's last, shorter chunk,
+// rounded up) at stored slots 128w + 4t + q.  tgt holds each block's position in the
+// item's row order (0xffff for the empty slots of the last chunk).  A thread loads its
+// four slots with one 128-bit load of their column ids, one of their targets and one per
+// block element plane, so every matrix byte moves in a coalesced load; and one gather
+// instruction of a warp reads x at 32 consecutive columns of the item (few cache lines).
+// The item's y rows are read with the blocks.  Each block's BH row products go to shared
+// memory at its target; then a lane group per block row adds its blocks in row order
+// (fixed shuffle tree) and writes y.  Work item descriptor: {first block row,
+// block rows | blocks << 16, first block in the source (row-pointer) numbering, first
+// stored slot}.
 constexpr int kGbThreads = 256;
 constexpr int kGbBlocks = 4 * kGbThreads;
 constexpr int kGbRows = 256;
 
+// Row sums of one item: a lane group of G lanes per block row adds the row's block
+// products (prod, row order) and writes y = s_y + sum (s_y: the item's y rows).
 template <int BH, int G>
-__device__ __forceinline__ void gb_rows(const int* s_rp, const float* prod, int br0, int nrows, int m,
+__device__ __forceinline__ void gb_rows(const int* s_rp, const float* prod, const float* s_y, int br0, int nrows, int m,
                                         float* __restrict__ y)
 {
     const int lane = threadIdx.x % G;
@@ -178,7 +183,7 @@ __device__ __forceinline__ void gb_rows(const int* s_rp, const float* prod, int 
         for (int h = 0; h < BH; h++) {
             const float t = group_sum<G>(acc[h]);
             const int r = (br0 + lr) * BH + h;
-            if (valid && lane == 0 && r < m) y[r] += t;
+            if (valid && lane == 0 && r < m) y[r] = s_y[lr * BH + h] + t;
         }
     }
 }
@@ -191,13 +196,13 @@ __global__ void __launch_bounds__(kGbThreads) bcsr_adaptive_kernel(const int* __
                                                                    int n)
 {
     __shared__ float prod[kGbBlocks * BH];
+    __shared__ float s_y[kGbRows * BH];
     __shared__ int s_rp[kGbRows + 1];
     const int4 wk = __ldg(work + blockIdx.x);
-    const int br0 = wk.x, nrows = wk.y, s = wk.z, e = wk.w;
-    const int s4 = s & ~3;
+    const int br0 = wk.x, nrows = wk.y & 0xffff, cnt = wk.y >> 16, s = wk.z;
     const int tid = threadIdx.x;
-    const int j = s4 + 4 * tid;
-    const bool act = j < e;
+    const int j = wk.w + 4 * tid;
+    const bool act = 4 * tid < cnt;
     int4 c = make_int4(0, 0, 0, 0);
     uint2 tg = make_uint2(0, 0);
     float4 d[BH * BW];
@@ -207,14 +212,18 @@ __global__ void __launch_bounds__(kGbThreads) bcsr_adaptive_kernel(const int* __
 #pragma unroll
         for (int k = 0; k < BH * BW; k++) d[k] = Val<V>::ld4(data + (size_t)k * aligned + j);
     }
-    if (tid < nrows) s_rp[tid] = __ldg(rp + br0 + tid) - s4;
-    if (tid == 0) s_rp[nrows] = e - s4;
+    // the item's row pointers and y rows, requested with the blocks so that the y update
+    // does not wait on DRAM
+    if (tid < nrows) s_rp[tid] = __ldg(rp + br0 + tid) - s;
+    if (tid == 0) s_rp[nrows] = cnt;
+    for (int i = tid; i < nrows * BH; i += kGbThreads)
+        if (br0 * BH + i < m) s_y[i] = y[br0 * BH + i];
     if (act) {
         const int cc[4] = {c.x, c.y, c.z, c.w};
         const int tq[4] = {(int)(tg.x & 0xffffu), (int)(tg.x >> 16), (int)(tg.y & 0xffffu), (int)(tg.y >> 16)};
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            const bool in = j + q >= s && j + q < e;
+            const bool in = tq[q] != 0xffff;
             float xv[BW];
 #pragma unroll
             for (int w = 0; w < BW; w++) xv[w] = (in && cc[q] + w < n) ? __ldg(x + cc[q] + w) : 0.0f;
@@ -227,16 +236,15 @@ __global__ void __launch_bounds__(kGbThreads) bcsr_adaptive_kernel(const int* __
                     const float a = q == 0 ? v.x : q == 1 ? v.y : q == 2 ? v.z : v.w;
                     t += a * xv[w];
                 }
-                // blocks of the previous item (before s) are skipped
                 if (in) prod[tq[q] * BH + h] = t;
             }
         }
     }
     __syncthreads();
-    if (nrows * 32 <= kGbThreads * 2) gb_rows<BH, 32>(s_rp, prod, br0, nrows, m, y);
-    else if (nrows * 8 <= kGbThreads * 2) gb_rows<BH, 8>(s_rp, prod, br0, nrows, m, y);
-    else if (nrows * 2 <= kGbThreads * 2) gb_rows<BH, 2>(s_rp, prod, br0, nrows, m, y);
-    else gb_rows<BH, 1>(s_rp, prod, br0, nrows, m, y);
+    if (nrows * 32 <= kGbThreads * 2) gb_rows<BH, 32>(s_rp, prod, s_y, br0, nrows, m, y);
+    else if (nrows * 8 <= kGbThreads * 2) gb_rows<BH, 8>(s_rp, prod, s_y, br0, nrows, m, y);
+    else if (nrows * 2 <= kGbThreads * 2) gb_rows<BH, 2>(s_rp, prod, s_y, br0, nrows, m, y);
+    else gb_rows<BH, 1>(s_rp, prod, s_y, br0, nrows, m, y);
 }
 
 }  // namespace dev
