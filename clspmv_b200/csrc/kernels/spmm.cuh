@@ -148,8 +148,10 @@ __global__ void __launch_bounds__(kSpmmThreads) bcsr_spmm4_kernel(const int* __r
             }
             __syncwarp(gmask);
             if (active) {
-                // U blocks of this sub-group at a time: their X rows are requested together
-                constexpr int U = (BW <= 3) ? 4 : 2;
+                // U blocks of this sub-group at a time: their X rows are requested together.
+                // With 8 float4 lanes (k >= 32), U = 2 keeps the kernel at 58 registers,
+                // 4 CTAs per SM; U = 4 took 80 and ran 17 % slower on 3x3 blocks at k = 32
+                constexpr int U = (BW <= 3 && CW < 8) ? 4 : 2;
                 for (int t0 = sub; t0 < nb; t0 += S * U) {
                     float4 xv[U][BW];
 #pragma unroll
