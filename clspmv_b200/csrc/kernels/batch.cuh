@@ -223,6 +223,7 @@ __device__ __forceinline__ void batch_sell(const BatchPart& P, int vb)
     const int* __restrict__ col = P.i1 + b + lr;
     const V* __restrict__ val = static_cast<const V*>(P.v) + b + lr;
     const float* __restrict__ x = P.x;
+    const float yo = P.y[r];   // requested with the first slots, not after the last
     float acc = 0.0f;
     const float yb = GRAD ? __ldg(P.ybar + r) : 0.0f;
     float* __restrict__ g = GRAD ? P.abar + b + lr : nullptr;
@@ -234,7 +235,7 @@ __device__ __forceinline__ void batch_sell(const BatchPart& P, int vb)
         acc += a * xv;
         if (GRAD) g[(size_t)k * H] = yb * xv;
     }
-    P.y[r] += acc;
+    P.y[r] = yo + acc;
 }
 
 // DIA rows [vb * 512, vb * 512 + 512): kBatchDiaRows rows per thread, 256 apart.
@@ -252,6 +253,7 @@ __device__ __forceinline__ void batch_dia(BatchSmem& sm, const BatchPart& P, int
     for (int i = 0; i < kBatchDiaRows; i++) {
         const int r = (vb * kBatchDiaRows + i) * kBatchThreads + threadIdx.x;
         if (r >= m) break;
+        const float yo = P.y[r];   // requested with the first diagonals, not after the last
         const float yb = GRAD ? __ldg(P.ybar + r) : 0.0f;
         float acc = 0.0f;
 #pragma unroll 4
@@ -262,7 +264,7 @@ __device__ __forceinline__ void batch_dia(BatchSmem& sm, const BatchPart& P, int
             acc += Val<V>::ld(val + (size_t)d * stride + r) * xv;
             if (GRAD) P.abar[(size_t)d * stride + r] = yb * xv;
         }
-        P.y[r] += acc;
+        P.y[r] = yo + acc;
     }
 }
 
@@ -283,6 +285,10 @@ __device__ __forceinline__ void batch_bcsr(const BatchPart& P, int vb)
 #pragma unroll
         for (int h = 0; h < B; h++) yb[h] = (valid && br * B + h < m) ? __ldg(P.ybar + br * B + h) : 0.0f;
     }
+    // the block row's y, requested with its first blocks, not after the last
+    float yo[B];
+#pragma unroll
+    for (int h = 0; h < B; h++) yo[h] = (valid && lane == 0 && br * B + h < m) ? P.y[br * B + h] : 0.0f;
     float acc[B];
 #pragma unroll
     for (int h = 0; h < B; h++) acc[h] = 0.0f;
@@ -309,7 +315,7 @@ __device__ __forceinline__ void batch_bcsr(const BatchPart& P, int vb)
     for (int h = 0; h < B; h++) {
         const float t = group_sum<G>(acc[h]);
         const int r = br * B + h;
-        if (valid && lane == 0 && r < m) P.y[r] += t;
+        if (valid && lane == 0 && r < m) P.y[r] = yo[h] + t;
     }
 }
 
