@@ -1,6 +1,6 @@
 """bench.py's output contract, checked on the host: the reference arm (the reference's
 serial csr_spmv, compiled from its own sources into oracle/_ref) prints one JSON line
-with the keys the harness reads; this library's arm has no CPU path and fails without a
+with the same metric, unit and keys as this library's arm; this library's arm has no CPU path and fails without a
 GPU; the per-partition DRAM traffic files that feed `roofline.traffic` are well formed."""
 import glob
 import json
@@ -27,9 +27,10 @@ def test_reference_arm_line():
     lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
     assert len(lines) == 1
     d = json.loads(lines[0])
-    base = json.load(open(os.path.join(ROOT, "BASELINE.json")))
+    sys.path.insert(0, ROOT)
+    import bench
     assert d["impl"] == "reference"
-    assert d["metric"] == base["metric"]
+    assert d["metric"] == bench.METRIC   # the same metric as this library's arm
     assert d["unit"] == "GB/s" and d["higher_is_better"] is True
     assert d["n_gpus"] == 1 and d["steps"] == 3 and d["warmup"] == 3
     assert d["value"] > 0 and d["ms_per_step"] > 0
