@@ -1,7 +1,7 @@
 /*
  * ORACLE -- test infrastructure only.  Never linked into, loaded by or called from
  * the product library or its Python package; only tests/, __graft_entry__.smoke()
- * and bench.py's CPU-baseline leg use it, as the checker.
+ * and bench.py's CPU-baseline leg use it, to check and to time against.
  *
  * A plain-C restatement of the reference's serial SpMV semantics
  * (clSpMV_NV/include/spmv_serial.h) plus an FP64 reference product and the
