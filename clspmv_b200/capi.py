@@ -167,6 +167,9 @@ class COO:
         self.s.coo_row_id = as_ptr(self.row, C.c_int)
         self.s.coo_col_id = as_ptr(self.col, C.c_int)
         self.s.coo_data = as_ptr(self.val, C.c_float)
+        # the struct holds the arrays its pointers reference: ref() of a temporary COO
+        # (`COO(...).ref()` passed straight to a call) keeps them alive through the call
+        self.s._arrays = (self.row, self.col, self.val)
 
     @property
     def nnz(self) -> int:

@@ -75,3 +75,42 @@ def test_spmm_rejects_other_formats():
     mat = Cocktail.single("coo", coo_of(case), 0)
     with pytest.raises(Exception, match="CSP_EUNSUP"):
         Handle(mat, None, None, nrhs=4)
+
+
+def _ragged(h, w, long_row, seed):
+    """Rows of 0-39 entries, 30 % of them empty, one row of `long_row` entries; h is not
+    a multiple of 2, 3 or 4, so the last block row is partial."""
+    rng = np.random.default_rng(seed)
+    lens = np.where(rng.random(h) < 0.3, 0, rng.integers(1, 40, h))
+    lens[h // 2] = long_row
+    rows, cols = [], []
+    for i, n in enumerate(lens):
+        if n:
+            rows.append(np.full(n, i, np.int32))
+            cols.append(np.sort(rng.choice(w, n, replace=False)).astype(np.int32))
+    r = np.concatenate(rows)
+    return h, w, r, np.concatenate(cols), rng.standard_normal(r.size).astype(np.float32)
+
+
+# 1,021 entries in one row: with 1x1 blocks exactly the largest work item of the single
+# right-hand-side kernel; 1,500: too long for one item (the row-per-group kernel runs)
+RAGGED = {"ragged": _ragged(10_007, 9_001, 1021, 84), "ragged_long": _ragged(10_007, 9_001, 1500, 85)}
+
+
+@pytest.mark.parametrize("name", sorted(RAGGED))
+@pytest.mark.parametrize("bs", [1, 2, 3, 4])
+@pytest.mark.parametrize("k", [1, 8])
+@pytest.mark.parametrize("bf16", [False, True])
+def test_generic_bcsr_ragged(name, bs, k, bf16):
+    """Empty block rows, a partial last block row and item-sized block rows."""
+    case = RAGGED[name]
+    h, w, r, c, v = case
+    b = capi.bcsr_matrix()
+    assert capi.lib().csp_coo2bcsr(coo_of(case).ref(), C.byref(b), bs, bs, 32) == 0
+    X, Y0 = _xy(h, w, k, seed=10)
+    hd = Handle(None, X, Y0, flags=CSP_FLAG_BF16 if bf16 else 0, nrhs=k, bcsr=b)
+    hd.do_spmv(1)
+    Y = hd.cpy_result_to_cpu()
+    hd.free()
+    capi.lib().csp_free_bcsr_matrix(C.byref(b))
+    _check_cols(case, Y, X, Y0, k, values=bf16_round(v) if bf16 else None)
