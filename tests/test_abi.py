@@ -55,3 +55,24 @@ def test_device_calls_fail_cleanly_without_gpu(L):
     rc = L.csp_init_mat_kernels(mat.ref(), capi.as_ptr(x, C.c_float), None, 0, C.byref(h))
     assert rc in (capi.CSP_ENODEV, capi.CSP_ECUDA)
     assert not h.value
+
+
+def test_temporary_coo_outlives_the_call(L):
+    """`COO(...).ref()` passed straight to a conversion: the struct keeps the arrays its
+    pointers reference alive through the call (large arrays, whose memory would
+    otherwise go back to the system at once)."""
+    rng = np.random.default_rng(5)
+    h, w, nnz = 200_000, 150_000, 1_000_000
+    r = np.sort(rng.integers(0, h, nnz)).astype(np.int32)
+    c = rng.integers(0, w, nnz).astype(np.int32)
+    v = rng.standard_normal(nnz).astype(np.float32)
+    ref = COO(h, w, r, c, v).ref()   # the COO itself is gone after this line
+    # freed arrays of these sizes would be handed out again here, and overwritten
+    junk = [np.full(nnz, 0x7fffffff, np.int32) for _ in range(2)] + [np.full(nnz, np.nan, np.float32)]
+    csr = capi.csr_matrix()
+    assert L.csp_coo2csr(ref, C.byref(csr)) == 0
+    del junk
+    rp = np.ctypeslib.as_array(csr.csr_row_ptr, (h + 1,)).copy()
+    assert rp[-1] == nnz
+    assert np.array_equal(np.diff(rp), np.bincount(r, minlength=h))
+    L.csp_free_csr_matrix(C.byref(csr))
