@@ -28,7 +28,7 @@ from .capi import (COO, CSP_ANALYZE_AUTOTUNE, CSP_ANALYZE_REFERENCE, CSP_FLAG_AD
 
 __all__ = ["COO", "Cocktail", "Handle", "analyze_matrix", "init_mat_kernels", "spmv_all", "evaluate",
            "CspError", "CSP_FLAG_BF16", "CSP_FLAG_GRAPH", "CSP_FLAG_USE_TEX", "CSP_FLAG_ADJOINT",
-           "CSP_FLAG_L2_PERSIST", "CSP_METH_XPANEL", "benchmark_tables", "gather_test",
+           "CSP_FLAG_L2_PERSIST", "CSP_METH_XPANEL", "benchmark_tables",
            "CSP_ANALYZE_REFERENCE", "CSP_ANALYZE_AUTOTUNE", "lib", "Batch"]
 
 from .batch import Batch  # noqa: E402
@@ -237,15 +237,6 @@ class Handle:
             self.free()
         except Exception:
             pass
-
-
-def gather_test() -> dict:
-    """Random 4-byte gather rates (elements/s) from L2-resident global memory, from a
-    CTA's shared memory and from a cluster's distributed shared memory (csp_gather_test)."""
-    r = capi.csp_gather_report()
-    check(lib().csp_gather_test(C.byref(r)), "gather_test")
-    return {"array_bytes": r.array_bytes, "l2_per_s": r.l2_per_s, "shared_per_s": r.shared_per_s,
-            "cluster_per_s": r.cluster_per_s}
 
 
 def benchmark_tables(clspmv_path: str, level: int = 1) -> None:

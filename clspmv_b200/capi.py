@@ -126,11 +126,6 @@ class csp_bandwidth_report(C.Structure):
                 ("gather_per_s", C.c_double)]
 
 
-class csp_gather_report(C.Structure):
-    _fields_ = [("array_bytes", C.c_double), ("l2_per_s", C.c_double), ("shared_per_s", C.c_double),
-                ("cluster_per_s", C.c_double)]
-
-
 class csp_report(C.Structure):
     _fields_ = [("method", C.c_int), ("gflops", C.c_double), ("gbytes", C.c_double), ("ms", C.c_double),
                 ("l2_distance", C.c_double), ("max_diff", C.c_double), ("max_ratio_diff", C.c_double),
@@ -231,7 +226,6 @@ def _declare(lib):
         "csp_read_mmf": (C.c_int, [C.c_char_p, P(coo_matrix)]),
         "csp_autotune_choice": (C.c_char_p, []),
         "csp_bandwidth_test": (C.c_int, [C.c_size_t, C.c_int, P(csp_bandwidth_report)]),
-        "csp_gather_test": (C.c_int, [P(csp_gather_report)]),
         "csp_spmv_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
         "csp_adjoint_slots": (C.c_int, [C.c_void_p, P(C.c_size_t)]),
         "csp_adjoint_pattern": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -15,8 +15,10 @@
 // reference's std::map and linear searches, which changes the cost on large
 // matrices but not the outcome.
 //
-// CSP_ANALYZE_AUTOTUNE runs the same partitioner on calibration tables measured on
-// the B200 by this library (see csp_write_b200_tables); a table path is required.
+// CSP_ANALYZE_AUTOTUNE does not use the tables: it hands the matrix to the on-device
+// autotuner (autotune.cu), which times candidate partitions on the GPU.  Tables
+// measured on the B200 by csp_benchmark_tables (calibrate.cu) can still drive the
+// reference partitioner through CSP_ANALYZE_REFERENCE and a table path.
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>

@@ -554,18 +554,6 @@ typedef struct csp_bandwidth_report {
 } csp_bandwidth_report;
 int csp_bandwidth_test(size_t bytes, int gather_range, csp_bandwidth_report* rep);
 
-/* Random 4-byte gather rates (elements per second) from a 1.5 MB global array (L2
- * resident), from one CTA's shared memory, and from the shared memory of an 8-CTA
- * thread-block cluster (distributed shared memory; -1 where clusters are not
- * available): the three places an SpMV kernel can read x from.  No counterpart in the
- * reference; a companion of spmv_all method 0. */
-typedef struct csp_gather_report {
-    double array_bytes;   /* size of the gathered array, bytes                 */
-    double l2_per_s;      /* global memory (L2 hits)                           */
-    double shared_per_s;  /* shared memory of the CTA                          */
-    double cluster_per_s; /* distributed shared memory of the cluster          */
-} csp_gather_report;
-int csp_gather_test(csp_gather_report* rep);
 
 /* ------------------------------------------------------------------------ */
 /* MatrixMarket input (fileio.cpp:10 ReadMMF): 0-based, pattern -> 1.0,       */

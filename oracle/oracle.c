@@ -169,19 +169,22 @@ void orc_sbell_spmv_f32(int height, int width, unsigned bw, unsigned bh, unsigne
 
 /*
  * FP64 reference product on CSR: out[r] = res0[r] + sum_j a_rj * vec[c_j], evaluated in
- * double, and bound[r] = |res0[r]| + sum_j |a_rj * vec[c_j]|, the scale of row r's
- * rounding error.  `transpose` != 0 computes A^T * vec instead (out has `width` rows):
- * the adjoint d(vec) = A^T * res_bar.
+ * double, and bound[r] = sum_j |a_rj * vec[c_j]| + res0_weight * |res0[r]|, the scale
+ * of row r's rounding error.  A test accepts row r when |y_r - out[r]| <= tol * bound[r];
+ * with tol = 1e-5 and res0_weight = 2^-23 / 1e-5 that is the FP32 bound
+ * 1e-5 * sum_j |a_rj x_j| + 2^-23 * |res0[r]| (the final FP32 add of res0 rounds by at
+ * most 2^-24 of the result).  `transpose` != 0 computes A^T * vec instead (out has
+ * `width` rows): the adjoint d(vec) = A^T * res_bar.
  */
 void orc_csr_spmv_f64(int height, int width, const int* row_ptr, const int* col, const float* val,
-                      const float* vec, const float* res0, int transpose,
+                      const float* vec, const float* res0, double res0_weight, int transpose,
                       double* out, double* bound)
 {
     int n_out = transpose ? width : height;
     for (int i = 0; i < n_out; i++) {
         double r0 = res0 ? (double)res0[i] : 0.0;
         out[i] = r0;
-        bound[i] = fabs(r0);
+        bound[i] = res0_weight * fabs(r0);
     }
     for (int r = 0; r < height; r++) {
         for (int j = row_ptr[r]; j < row_ptr[r + 1]; j++) {
@@ -195,6 +198,21 @@ void orc_csr_spmv_f64(int height, int width, const int* row_ptr, const int* col,
                 bound[col[j]] += fabs(p);
             }
         }
+    }
+}
+
+/*
+ * Value gradient of y = A x on the CSR pattern: abar[j] = res_bar[row(j)] * vec[col[j]]
+ * (the derivative of y_row with respect to a_row,col, weighted by res_bar).  The
+ * reference has no adjoint; this is the definition, used to time a CPU counterpart of
+ * the device's gradient pass.
+ */
+void orc_csr_value_grad_f32(int height, const int* row_ptr, const int* col, const float* res_bar,
+                            const float* vec, float* abar)
+{
+    for (int r = 0; r < height; r++) {
+        float yb = res_bar[r];
+        for (int j = row_ptr[r]; j < row_ptr[r + 1]; j++) abar[j] = yb * vec[col[j]];
     }
 }
 

@@ -25,7 +25,8 @@ def oracle_lib():
         if not os.path.exists(ORACLE):
             raise RuntimeError("oracle/liboracle.so missing: run `make -C oracle`")
         l = C.CDLL(ORACLE)
-        l.orc_csr_spmv_f64.argtypes = [C.c_int, C.c_int, IP, IP, FP, FP, FP, C.c_int, DP, DP]
+        l.orc_csr_spmv_f64.argtypes = [C.c_int, C.c_int, IP, IP, FP, FP, FP, C.c_double, C.c_int, DP, DP]
+        l.orc_csr_value_grad_f32.argtypes = [C.c_int, IP, IP, FP, FP, FP]
         l.orc_max_rel_err.argtypes = [C.c_int, FP, DP, DP, IP]
         l.orc_max_rel_err.restype = C.c_double
         l.orc_csr_spmv_f32.argtypes = [C.c_int, IP, IP, FP, FP, FP]
@@ -84,8 +85,16 @@ def ref_lib():
     return _ref
 
 
-def fp64_spmv(h, w, rp, col, val, x, y0=None, transpose=False):
-    """FP64 reference product and per-row error scale |y0| + sum |a_ij x_j|."""
+# The per-row FP32 bound the parity tests apply: |y_i - yhat_i| <= TOL * bound_i with
+# bound_i = sum_j |a_ij x_j| + Y0_WEIGHT * |y0_i|, i.e. 1e-5 * sum_j |a_ij x_j| plus
+# 2^-23 * |y0_i| for the final FP32 add of the accumulated vector.
+TOL = 1e-5
+Y0_WEIGHT = 2.0 ** -23 / TOL
+
+
+def fp64_spmv(h, w, rp, col, val, x, y0=None, transpose=False, y0_weight=Y0_WEIGHT):
+    """FP64 reference product y0 + A x (or A^T x) and the per-row error scale
+    sum_j |a_ij x_j| + y0_weight * |y0_i|."""
     l = oracle_lib()
     rp = np.ascontiguousarray(rp, np.int32)
     col = np.ascontiguousarray(col, np.int32)
@@ -99,9 +108,14 @@ def fp64_spmv(h, w, rp, col, val, x, y0=None, transpose=False):
     out = np.zeros(n_out, np.float64)
     bound = np.zeros(n_out, np.float64)
     l.orc_csr_spmv_f64(h, w, rp.ctypes.data_as(IP), col.ctypes.data_as(IP), val.ctypes.data_as(FP),
-                       x.ctypes.data_as(FP), y0p, 1 if transpose else 0, out.ctypes.data_as(DP),
+                       x.ctypes.data_as(FP), y0p, float(y0_weight), 1 if transpose else 0, out.ctypes.data_as(DP),
                        bound.ctypes.data_as(DP))
     return out, bound
+
+
+def y0_term(y0, adds: int = 1):
+    """The bound's share for an accumulated vector y0 that `adds` FP32 additions update."""
+    return Y0_WEIGHT * adds * np.abs(np.asarray(y0, np.float64))
 
 
 def max_rel_err(y, yhat, bound):

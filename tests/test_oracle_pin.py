@@ -106,7 +106,7 @@ def test_fp64_oracle_against_numpy(orc):
     dense[r, c] = v
     want = y0.astype(np.float64) + dense @ x.astype(np.float64)
     assert np.allclose(out, want, rtol=0, atol=1e-12)
-    assert np.allclose(bound, np.abs(y0) + np.abs(dense) @ np.abs(x.astype(np.float64)), atol=1e-12)
+    assert np.allclose(bound, _oracle.Y0_WEIGHT * np.abs(y0) + np.abs(dense) @ np.abs(x.astype(np.float64)), atol=1e-12)
     outt, _ = _oracle.fp64_spmv(h, w, rp, c, v, y0, None, transpose=True)
     assert np.allclose(outt, dense.T @ y0.astype(np.float64), atol=1e-12)
 
