@@ -23,12 +23,12 @@ import numpy as np
 
 from . import capi
 from .capi import (COO, CSP_ANALYZE_AUTOTUNE, CSP_ANALYZE_REFERENCE, CSP_FLAG_ADJOINT, CSP_FLAG_BF16,
-                   CSP_FLAG_L2_PERSIST, CSP_METH_XPANEL,
+                   CSP_FLAG_L2_PERSIST, CSP_FLAG_TENSOR_CORES, CSP_METH_XPANEL,
                    CSP_FLAG_GRAPH, CSP_FLAG_USE_TEX, CspError, check, lib, to_numpy)
 
 __all__ = ["COO", "Cocktail", "Handle", "analyze_matrix", "init_mat_kernels", "spmv_all", "evaluate",
            "CspError", "CSP_FLAG_BF16", "CSP_FLAG_GRAPH", "CSP_FLAG_USE_TEX", "CSP_FLAG_ADJOINT",
-           "CSP_FLAG_L2_PERSIST", "CSP_METH_XPANEL", "benchmark_tables",
+           "CSP_FLAG_L2_PERSIST", "CSP_FLAG_TENSOR_CORES", "CSP_METH_XPANEL", "benchmark_tables",
            "CSP_ANALYZE_REFERENCE", "CSP_ANALYZE_AUTOTUNE", "lib", "Batch"]
 
 from .batch import Batch  # noqa: E402

@@ -20,6 +20,7 @@ FP = C.POINTER(C.c_float)
 
 CSP_OK, CSP_EINVAL, CSP_ENOMEM, CSP_ECUDA, CSP_EFORMAT, CSP_ENODEV, CSP_EUNSUP, CSP_EIO, CSP_ETIMEOUT = range(9)
 CSP_FLAG_USE_TEX, CSP_FLAG_BF16, CSP_FLAG_GRAPH, CSP_FLAG_ADJOINT, CSP_FLAG_L2_PERSIST = 0x1, 0x2, 0x4, 0x8, 0x10
+CSP_FLAG_TENSOR_CORES = 0x20
 CSP_METH_XPANEL = 16
 CSP_ANALYZE_REFERENCE, CSP_ANALYZE_AUTOTUNE = 0, 1
 CSP_NOALLOC_MAX_NNZ = 33554432

@@ -28,6 +28,80 @@ namespace {
 
 struct Entry { int r, c; float v; };
 
+// Every stored slot of a b4 block layout (matrix_storage.h:2203 SBELL, :2010 BELL,
+// :1741 BCSR): f(i, row, col) with i the slot's index in the part's data array and
+// row -1 where the slot lies outside the matrix (alignment rows and columns).
+template <class F> void for_each_sbell_slot(const sbell_matrix_if& s, F f)
+{
+    const int bw = (int)s.sbell_bwidth, bh = (int)s.sbell_bheight, sh = (int)s.sbell_slice_height, bw4 = bw / 4;
+    const size_t total = (size_t)s.sbell_slice_ptr[s.sbell_slice_num] * bw * bh;
+    std::vector<char> seen(total, 0);
+    for (int br = 0; br < s.sbell_row_num; br++) {
+        const int sl = br / sh, lr = br % sh;
+        const int cs = s.sbell_slice_ptr[sl];
+        const int width = (s.sbell_slice_ptr[sl + 1] - cs) / sh;
+        for (int k = 0; k < width; k++) {
+            const int c4 = s.sbell_col_id[cs + lr + k * sh];
+            for (int h = 0; h < bh; h++)
+                for (int w4 = 0; w4 < bw4; w4++)
+                    for (int w = 0; w < 4; w++) {
+                        const size_t i = (size_t)cs * bw * bh + (size_t)k * sh * bw4 * bh * 4 + (size_t)h * sh * 4 +
+                                         (size_t)w4 * sh * bh * 4 + (size_t)lr * 4 + w;
+                        const int r = br * bh + h, c = (c4 + w4) * 4 + w;
+                        const bool in = r < s.matinfo.height && c < s.matinfo.width;
+                        f(i, in ? r : -1, in ? c : -1);
+                        seen[i] = 1;
+                    }
+        }
+    }
+    for (size_t i = 0; i < total; i++)
+        if (!seen[i]) f(i, -1, -1);   // slice rows past the last block row
+}
+
+template <class F> void for_each_bell_slot(const b4ell_matrix_if& b, F f)
+{
+    const int bw4 = (int)b.b4ell_bwidth / 4, bh = (int)b.b4ell_bheight, f4 = b.b4ell_float4_aligned;
+    const size_t total = (size_t)f4 * bh * bw4 * b.b4ell_block_num;
+    std::vector<char> seen(total, 0);
+    for (int br = 0; br < b.b4ell_row_num; br++)
+        for (int k = 0; k < b.b4ell_block_num; k++) {
+            const int c4 = b.b4ell_col_id[(size_t)k * b.b4ell_height_aligned + br];
+            for (int h = 0; h < bh; h++)
+                for (int w4 = 0; w4 < bw4; w4++)
+                    for (int w = 0; w < 4; w++) {
+                        const size_t i = (size_t)k * f4 * bw4 * bh + (size_t)h * f4 + (size_t)w4 * f4 * bh + (size_t)br * 4 + w;
+                        const int r = br * bh + h, c = (c4 + w4) * 4 + w;
+                        const bool in = r < b.matinfo.height && c < b.matinfo.width;
+                        f(i, in ? r : -1, in ? c : -1);
+                        seen[i] = 1;
+                    }
+        }
+    for (size_t i = 0; i < total; i++)
+        if (!seen[i]) f(i, -1, -1);   // alignment block rows
+}
+
+template <class F> void for_each_bcsr_slot(const b4csr_matrix_if& b, F f)
+{
+    const int bw4 = (int)b.b4csr_bwidth / 4, bh = (int)b.b4csr_bheight, al = b.b4csr_aligned_size;
+    const size_t total = (size_t)al * bh * bw4;
+    std::vector<char> seen(total, 0);
+    for (int br = 0; br < b.b4csr_row_num; br++)
+        for (int j = b.b4csr_row_ptr[br]; j < b.b4csr_row_ptr[br + 1]; j++) {
+            const int c4 = b.b4csr_col_id[j];
+            for (int h = 0; h < bh; h++)
+                for (int w4 = 0; w4 < bw4; w4++)
+                    for (int w = 0; w < 4; w++) {
+                        const size_t i = (size_t)w4 * al * bh + (size_t)h * al + (size_t)j * 4 + w;
+                        const int r = br * bh + h, c = (c4 + w4) * 4 + w;
+                        const bool in = r < b.matinfo.height && c < b.matinfo.width;
+                        f(i, in ? r : -1, in ? c : -1);
+                        seen[i] = 1;
+                    }
+        }
+    for (size_t i = 0; i < total; i++)
+        if (!seen[i]) f(i, -1, -1);   // alignment slots past the last block
+}
+
 // Nonzeros of the non-diagonal parts of `mat`, gathered from their host layouts.
 void gather_entries(const cocktail_iif* mat, bool include_diag, std::vector<Entry>& out)
 {
@@ -53,56 +127,10 @@ void gather_entries(const cocktail_iif* mat, bool include_diag, std::vector<Entr
                 }
             }
     }
-    if (mat->ifusesbell) {
-        const sbell_matrix_if& s = mat->sbell;
-        const int bw = (int)s.sbell_bwidth, bh = (int)s.sbell_bheight, sh = (int)s.sbell_slice_height, bw4 = bw / 4;
-        for (int br = 0; br < s.sbell_row_num; br++) {
-            const int sl = br / sh, lr = br % sh;
-            const int cs = s.sbell_slice_ptr[sl];
-            const int width = (s.sbell_slice_ptr[sl + 1] - cs) / sh;
-            for (int k = 0; k < width; k++) {
-                const int c4 = s.sbell_col_id[cs + lr + k * sh];
-                for (int h = 0; h < bh; h++)
-                    for (int w4 = 0; w4 < bw4; w4++)
-                        for (int w = 0; w < 4; w++) {
-                            const size_t i = (size_t)cs * bw * bh + (size_t)k * sh * bw4 * bh * 4 + (size_t)h * sh * 4 +
-                                             (size_t)w4 * sh * bh * 4 + (size_t)lr * 4 + w;
-                            const int r = br * bh + h, c = (c4 + w4) * 4 + w;
-                            if (r < s.matinfo.height && c < s.matinfo.width) add(r, c, s.sbell_data[i]);
-                        }
-            }
-        }
-    }
-    if (mat->ifusebell) {
-        const b4ell_matrix_if& b = mat->bell;
-        const int bw4 = (int)b.b4ell_bwidth / 4, bh = (int)b.b4ell_bheight, f4 = b.b4ell_float4_aligned;
-        for (int br = 0; br < b.b4ell_row_num; br++)
-            for (int k = 0; k < b.b4ell_block_num; k++) {
-                const int c4 = b.b4ell_col_id[(size_t)k * b.b4ell_height_aligned + br];
-                for (int h = 0; h < bh; h++)
-                    for (int w4 = 0; w4 < bw4; w4++)
-                        for (int w = 0; w < 4; w++) {
-                            const size_t i = (size_t)k * f4 * bw4 * bh + (size_t)h * f4 + (size_t)w4 * f4 * bh + (size_t)br * 4 + w;
-                            const int r = br * bh + h, c = (c4 + w4) * 4 + w;
-                            if (r < b.matinfo.height && c < b.matinfo.width) add(r, c, b.b4ell_data[i]);
-                        }
-            }
-    }
-    if (mat->ifusebcsr) {
-        const b4csr_matrix_if& b = mat->bcsr;
-        const int bw4 = (int)b.b4csr_bwidth / 4, bh = (int)b.b4csr_bheight, al = b.b4csr_aligned_size;
-        for (int br = 0; br < b.b4csr_row_num; br++)
-            for (int j = b.b4csr_row_ptr[br]; j < b.b4csr_row_ptr[br + 1]; j++) {
-                const int c4 = b.b4csr_col_id[j];
-                for (int h = 0; h < bh; h++)
-                    for (int w4 = 0; w4 < bw4; w4++)
-                        for (int w = 0; w < 4; w++) {
-                            const size_t i = (size_t)w4 * al * bh + (size_t)h * al + (size_t)j * 4 + w;
-                            const int r = br * bh + h, c = (c4 + w4) * 4 + w;
-                            if (r < b.matinfo.height && c < b.matinfo.width) add(r, c, b.b4csr_data[i]);
-                        }
-            }
-    }
+    auto add_slot = [&](size_t i, int r, int c, const float* data) { if (r >= 0) add(r, c, data[i]); };
+    if (mat->ifusesbell) for_each_sbell_slot(mat->sbell, [&](size_t i, int r, int c) { add_slot(i, r, c, mat->sbell.sbell_data); });
+    if (mat->ifusebell) for_each_bell_slot(mat->bell, [&](size_t i, int r, int c) { add_slot(i, r, c, mat->bell.b4ell_data); });
+    if (mat->ifusebcsr) for_each_bcsr_slot(mat->bcsr, [&](size_t i, int r, int c) { add_slot(i, r, c, mat->bcsr.b4csr_data); });
     if (mat->ifusesell) {
         const sell_matrix_if& s = mat->sell;
         const int H = (int)s.sell_slice_height;
@@ -151,6 +179,85 @@ void transpose_dia(int n, int len, const std::vector<int>& off, const float* dat
 }
 
 }  // namespace
+
+// A value-gradient segment given by the (row, col) of each slot (row -1: padding).
+int Engine::add_slot_list(Seg& s, const std::vector<int>& rows, const std::vector<int>& cols)
+{
+    int *d_r = nullptr, *d_c = nullptr;
+    int rc;
+    if ((rc = upload_int(&d_r, rows.data(), rows.size(), std::max<size_t>(rows.size(), 1))) ||
+        (rc = upload_int(&d_c, cols.data(), cols.size(), std::max<size_t>(cols.size(), 1))))
+        return rc;
+    s.kind = SEG_LIST;
+    s.a0 = d_r;
+    s.a1 = d_c;
+    s.count = rows.size();
+    return CSP_OK;
+}
+
+// Adjoint of a generic BCSR handle (csp_init_bcsr_kernels with CSP_FLAG_ADJOINT): A^T
+// as one transposed CSR part of the blocks' nonzeros, and value gradients over every
+// slot of the caller's BCSR layout (data[e * aligned + block], matrix_storage.h:1595),
+// element e of a block being row e / bw, column e % bw; alignment slots, and slots
+// of a partial last block row or column, get row -1.
+int Engine::build_adjoint_gbcsr(const bcsr_matrix_if& b)
+{
+    adjoint = true;
+    const int bw = (int)b.bcsr_bwidth, bh = (int)b.bcsr_bheight, al = b.bcsr_aligned_size, nb = b.bcsr_block_num;
+    std::vector<Entry> e;
+    std::vector<int> brow((size_t)std::max(nb, 1), -1);
+    for (int br = 0; br < b.bcsr_row_num; br++)
+        for (int j = b.bcsr_row_ptr[br]; j < b.bcsr_row_ptr[br + 1]; j++) {
+            brow[j] = br;
+            for (int q = 0; q < bh * bw; q++) {
+                const int r = br * bh + q / bw, c = b.bcsr_col_id[j] + q % bw;
+                const float v = b.bcsr_data[(size_t)q * al + j];
+                if (r < height && c < width && v != 0.0f) e.push_back(Entry{r, c, v});
+            }
+        }
+    int rc = CSP_OK;
+    std::swap(width, height);
+    std::swap(parts, adj_parts);
+    if (!e.empty()) {
+        std::stable_sort(e.begin(), e.end(), [](const Entry& p, const Entry& q) { return p.c != q.c ? p.c < q.c : p.r < q.r; });
+        csr_matrix_if t;
+        csp_init_csr_matrix(&t);
+        std::vector<int> rp((size_t)height + 1, 0), col(e.size());
+        std::vector<float> val(e.size());
+        for (size_t i = 0; i < e.size(); i++) {
+            rp[(size_t)e[i].c + 1]++;
+            col[i] = e[i].r;
+            val[i] = e[i].v;
+        }
+        for (int i = 0; i < height; i++) rp[i + 1] += rp[i];
+        t.matinfo.width = width;
+        t.matinfo.height = height;
+        t.matinfo.nnz = (int)e.size();
+        t.csr_row_ptr = rp.data();
+        t.csr_col_id = col.data();
+        t.csr_data = val.data();
+        rc = add_csr(t, 2);
+    }
+    std::swap(parts, adj_parts);
+    std::swap(width, height);
+    if (rc) return rc;
+    Seg s;
+    s.offset = 0;
+    int *d_brow = nullptr, *d_col = nullptr;
+    if ((rc = upload_int(&d_brow, brow.data(), (size_t)nb, std::max<size_t>(nb, 1))) ||
+        (rc = upload_int(&d_col, b.bcsr_col_id, (size_t)nb, std::max<size_t>(nb, 1))))
+        return rc;
+    s.kind = SEG_GBCSR;
+    s.a0 = d_brow;
+    s.a1 = d_col;
+    s.p0 = al;
+    s.p1 = nb;
+    s.p2 = bh * 16 + bw;
+    s.count = (size_t)al * bh * bw;
+    segs.push_back(s);
+    abar_total = s.count;
+    return CSP_OK;
+}
 
 int Engine::build_adjoint(const cocktail_iif* mat)
 {
@@ -315,8 +422,24 @@ int Engine::build_adjoint(const cocktail_iif* mat)
             s.p2 = p.m;
             s.count = (size_t)mat->sell.sell_slice_ptr[mat->sell.sell_slice_num];
             break;
+        case PART_SBELL:
+        case PART_BELL:
+        case PART_BCSR: {
+            // block layouts: the (row, col) of every slot, row -1 for padding
+            std::vector<int> rows, cols;
+            auto put = [&](size_t i, int r, int c) {
+                if (i >= rows.size()) { rows.resize(i + 1, -1); cols.resize(i + 1, -1); }
+                rows[i] = r;
+                cols[i] = c;
+            };
+            if (p.kind == PART_SBELL) for_each_sbell_slot(mat->sbell, put);
+            else if (p.kind == PART_BELL) for_each_bell_slot(mat->bell, put);
+            else for_each_bcsr_slot(mat->bcsr, put);
+            if ((rc = add_slot_list(s, rows, cols))) return rc;
+            break;
+        }
         default:
-            s.kind = SEG_NONE;   // block formats: value gradients not provided
+            s.kind = SEG_NONE;
             s.count = 0;
             abar_blocks = true;
             break;
@@ -345,7 +468,11 @@ int Engine::launch_abar(const float* ybar, float* abar, int* prow, int* pcol, cu
                 abar_dia_kernel<<<g, 256, 0, st>>>(s.a0, s.p0, s.p1, s.p2, width, ybar, d_x, a, pr, pc);
             }
             break;
-        case SEG_LIST: abar_list_kernel<<<g, 256, 0, st>>>(s.a0, s.a1, s.p0, ybar, d_x, a, pr, pc); break;
+        case SEG_LIST: abar_list_kernel<<<g, 256, 0, st>>>(s.a0, s.a1, s.count, ybar, d_x, a, pr, pc); break;
+        case SEG_GBCSR:
+            abar_gbcsr_kernel<<<g, 256, 0, st>>>(s.a0, s.a1, s.p0, s.p1, s.p2 >> 4, s.p2 & 15, height, width, ybar, d_x, a,
+                                                 pr, pc);
+            break;
         case SEG_ELL: abar_ell_kernel<<<g, 256, 0, st>>>(s.a0, s.p0, s.p1, s.p2, ybar, d_x, a, pr, pc); break;
         case SEG_SELL: {
             const unsigned gs = (unsigned)(((size_t)s.p1 * s.p0 + 255) / 256);
@@ -371,7 +498,7 @@ int csp_spmv_adjoint(csp_handle* h, const float* d_ybar, float* d_xbar, float* d
     csp::Engine& e = h->eng;
     if (!e.adjoint) return set_error(CSP_EINVAL, "handle was not built with CSP_FLAG_ADJOINT");
     if (!d_ybar) return set_error(CSP_EINVAL, "null ybar");
-    if (d_abar && e.abar_blocks) return set_error(CSP_EUNSUP, "value gradients of block-format parts are not provided");
+    if (d_abar && e.abar_blocks) return set_error(CSP_EUNSUP, "value gradients of this handle's parts are not provided");
     if (d_xbar) {
         int rc = e.enqueue_parts(e.adj_parts, d_ybar, d_xbar, e.height, e.stream);
         if (rc) return rc;
@@ -392,7 +519,7 @@ int csp_adjoint_pattern(csp_handle* h, int* d_rows, int* d_cols)
 {
     if (!h || !d_rows || !d_cols) return set_error(CSP_EINVAL, "null argument");
     if (!h->eng.adjoint) return set_error(CSP_EINVAL, "handle was not built with CSP_FLAG_ADJOINT");
-    if (h->eng.abar_blocks) return set_error(CSP_EUNSUP, "value gradients of block-format parts are not provided");
+    if (h->eng.abar_blocks) return set_error(CSP_EUNSUP, "value gradients of this handle's parts are not provided");
     return h->eng.launch_abar(nullptr, nullptr, d_rows, d_cols, h->eng.stream);
 }
 

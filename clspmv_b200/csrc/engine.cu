@@ -683,10 +683,24 @@ int Engine::add_generic_bcsr(const bcsr_matrix_if& b, int method)
 // Launches
 // --------------------------------------------------------------------------
 template <class V>
-static void launch_spmm(const Part& p, const float* x, float* y, int n, int k, cudaStream_t st)
+static void launch_spmm(const Part& p, const float* x, float* y, int n, int k, bool tensor, cudaStream_t st)
 {
     using namespace dev;
     const V* v = static_cast<const V*>(p.v);
+    if (tensor && p.kind == PART_GBCSR && k % 32 == 0 && p.bh <= 8 && p.bw <= 4) {
+        // tensor cores: one warp per block row, two blocks per MMA step
+        if (p.nbr == 0) return;
+        const unsigned g = grid_for((long long)p.nbr * 32, kMmaThreads);
+#define CSP_MMA(BH, BW) \
+    bcsr_spmm_mma_kernel<V, BH, BW, 2><<<g, kMmaThreads, 0, st>>>(p.i0, p.i1, v, x, y, p.nbr, p.stride, p.m, n, k)
+        switch (p.bh * 10 + p.bw) {
+        case 11: CSP_MMA(1, 1); break; case 22: CSP_MMA(2, 2); break; case 33: CSP_MMA(3, 3); break;
+        case 44: CSP_MMA(4, 4); break;
+        default: break;
+        }
+#undef CSP_MMA
+        if (p.bh * 10 + p.bw == 11 || p.bh * 10 + p.bw == 22 || p.bh * 10 + p.bw == 33 || p.bh * 10 + p.bw == 44) return;
+    }
     const int G = k >= 32 ? 32 : (k > 16 ? 32 : (k > 8 ? 16 : (k > 4 ? 8 : (k > 2 ? 4 : 2))));
     if (p.kind == PART_CSR) {
         if (p.m == 0) return;
@@ -884,8 +898,8 @@ int Engine::enqueue_parts(const std::vector<Part>& ps, const float* x, float* y,
 {
     for (const Part& p : ps) {
         if (nrhs > 1) {
-            if (bf16) launch_spmm<__nv_bfloat16>(p, x, y, n, nrhs, st);
-            else launch_spmm<float>(p, x, y, n, nrhs, st);
+            if (bf16) launch_spmm<__nv_bfloat16>(p, x, y, n, nrhs, tensor_spmm, st);
+            else launch_spmm<float>(p, x, y, n, nrhs, tensor_spmm, st);
         } else {
             if (bf16) launch_part<__nv_bfloat16>(p, x, y, n, st);
             else launch_part<float>(p, x, y, n, st);
@@ -1024,6 +1038,7 @@ int Engine::init_common(int w, int h, int nz, const float* vec, const float* res
     nrhs = k;
     bf16 = (flags & CSP_FLAG_BF16) != 0;
     use_graph = (flags & CSP_FLAG_GRAPH) != 0;
+    tensor_spmm = (flags & CSP_FLAG_TENSOR_CORES) != 0;
     int ndev = 0;
     cudaError_t e = cudaGetDeviceCount(&ndev);
     if (e != cudaSuccess || ndev == 0) return set_error(CSP_ENODEV, "no CUDA device: %s", cudaGetErrorString(e));
@@ -1074,11 +1089,12 @@ int Engine::init(const cocktail_iif* mat, const float* vec, const float* res, in
 int Engine::init_bcsr(const bcsr_matrix_if* b, const float* vec, const float* res, int flags, int k)
 {
     if (!b) return set_error(CSP_EINVAL, "null BCSR");
-    if (flags & CSP_FLAG_ADJOINT) return set_error(CSP_EUNSUP, "adjoint of a generic BCSR handle");
+    if ((flags & CSP_FLAG_ADJOINT) && k > 1) return set_error(CSP_EUNSUP, "adjoint with several right-hand sides");
     if (k > 1 && b->bcsr_bwidth * b->bcsr_bheight > 36) return set_error(CSP_EUNSUP, "several right-hand sides need blocks of <= 36 elements");
     int rc = init_common(b->matinfo.width, b->matinfo.height, b->matinfo.nnz, vec, res, flags, k);
     if (rc) return rc;
     if ((rc = add_generic_bcsr(*b, 0))) return rc;
+    if ((flags & CSP_FLAG_ADJOINT) && (rc = build_adjoint_gbcsr(*b))) return rc;
     CSP_CUDA(cudaDeviceSynchronize());
     return CSP_OK;
 }

@@ -50,7 +50,7 @@ struct Part {
     bool from_csr = false;            // adjoint: value-gradient order follows the CSR part
 };
 
-enum SegKind { SEG_NONE, SEG_DIA, SEG_LIST, SEG_ELL, SEG_SELL };
+enum SegKind { SEG_NONE, SEG_DIA, SEG_LIST, SEG_ELL, SEG_SELL, SEG_GBCSR };
 
 // One forward part's share of the value-gradient array (adjoint).
 struct Seg {
@@ -66,6 +66,7 @@ struct Engine {
     int nrhs = 1;            // right-hand sides: x is width x nrhs, y height x nrhs, row-major
     bool bf16 = false;
     bool use_graph = false;
+    bool tensor_spmm = false;   // CSP_FLAG_TENSOR_CORES
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     float* d_x = nullptr;
@@ -82,7 +83,7 @@ struct Engine {
     static constexpr int kIterChunk = 32;
     // adjoint (CSP_FLAG_ADJOINT)
     bool adjoint = false;
-    bool abar_blocks = false;          // a block-format part: no value gradients
+    bool abar_blocks = false;          // a part without value gradients (none of the built formats)
     std::vector<Part> adj_parts;       // parts of A^T: xbar += A^T ybar
     std::vector<Seg> segs;
     size_t abar_total = 0;
@@ -98,6 +99,8 @@ struct Engine {
     int enqueue_once(cudaStream_t st);
     int enqueue_parts(const std::vector<Part>& ps, const float* x, float* y, int n, cudaStream_t st);
     int build_adjoint(const cocktail_iif* mat);
+    int build_adjoint_gbcsr(const bcsr_matrix_if& b);
+    int add_slot_list(Seg& s, const std::vector<int>& rows, const std::vector<int>& cols);
     int launch_abar(const float* ybar, float* abar, int* prow, int* pcol, cudaStream_t st);
     int launches_per_spmv() const;
 

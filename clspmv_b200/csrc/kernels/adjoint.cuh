@@ -80,15 +80,36 @@ __global__ void __launch_bounds__(256) abar_dia4_kernel(const int* __restrict__ 
     }
 }
 
-// Entry lists with explicit row ids (COO; CSR with its row-id array).
-__global__ void __launch_bounds__(256) abar_list_kernel(const int* __restrict__ rows, const int* __restrict__ cols, int nnz,
-                                                        const float* __restrict__ ybar, const float* __restrict__ x,
-                                                        float* __restrict__ abar, int* __restrict__ prow,
-                                                        int* __restrict__ pcol)
+// Slot lists with explicit row ids (COO; CSR with its row-id array; the block layouts'
+// slot maps, row -1 on padding slots).
+__global__ void __launch_bounds__(256) abar_list_kernel(const int* __restrict__ rows, const int* __restrict__ cols,
+                                                        size_t nslots, const float* __restrict__ ybar,
+                                                        const float* __restrict__ x, float* __restrict__ abar,
+                                                        int* __restrict__ prow, int* __restrict__ pcol)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nnz) return;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nslots) return;
     put_slot(i, __ldg(rows + i), __ldg(cols + i), ybar, x, abar, prow, pcol);
+}
+
+// Generic BCSR slots data[e * aligned + j]: element e of block j couples row
+// brow[j] * bh + e / bw with column col[j] + e % bw (row -1 past the blocks or the matrix).
+__global__ void __launch_bounds__(256) abar_gbcsr_kernel(const int* __restrict__ brow, const int* __restrict__ col,
+                                                         int aligned, int nblocks, int bh, int bw, int m, int n,
+                                                         const float* __restrict__ ybar, const float* __restrict__ x,
+                                                         float* __restrict__ abar, int* __restrict__ prow,
+                                                         int* __restrict__ pcol)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (size_t)aligned * bh * bw) return;
+    const int e = (int)(i / aligned), j = (int)(i % aligned);
+    int r = -1, c = -1;
+    if (j < nblocks) {
+        r = __ldg(brow + j) * bh + e / bw;
+        c = __ldg(col + j) + e % bw;
+        if (r >= m || c >= n) r = -1;
+    }
+    put_slot(i, r, c, ybar, x, abar, prow, pcol);
 }
 
 // Column-major ELL slots (k, r), r < height_aligned.

@@ -171,7 +171,8 @@ __global__ void __launch_bounds__(256) coo_noalloc_fixup(const int* __restrict__
     if (r >= 0 && r < height) y[r] += acc;
 }
 
-// Device address of g_noalloc_scratch, looked up once per device with that device current.
+// Device address of g_noalloc_scratch, looked up once per device with that device
+// current and kept for the process (a cudaDeviceReset afterwards is not supported).
 constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mutex;
 void* g_scratch_addr[kMaxDevices];
@@ -206,6 +207,13 @@ extern "C" int csp_coo_spmv_noalloc(int height, int width, int nnz, const int* d
                          nnz, CSP_NOALLOC_MAX_NNZ);
     if (nnz == 0) return CSP_OK;
     if (!d_row || !d_col || !d_val || !d_x || !d_y) return set_error(CSP_EINVAL, "coo_spmv_noalloc: null device pointer");
+    {
+        // x is read while y is written: the arrays must not overlap
+        const uintptr_t x0 = (uintptr_t)d_x, x1 = x0 + sizeof(float) * (size_t)width;
+        const uintptr_t y0 = (uintptr_t)d_y, y1 = y0 + sizeof(float) * (size_t)height;
+        if (x0 < y1 && y0 < x1 && width > 0 && height > 0)
+            return set_error(CSP_EINVAL, "coo_spmv_noalloc: x and y overlap");
+    }
     if (((uintptr_t)d_row | (uintptr_t)d_col | (uintptr_t)d_val) & 15)
         return set_error(CSP_EINVAL, "coo_spmv_noalloc: row, column and value arrays must be 16-byte aligned");
     void* scratch = nullptr;

@@ -324,6 +324,10 @@ typedef struct csp_handle csp_handle;
                                     the handle's own stream, with persisting L2 reserved for this process's
                                     context up to x's size; not applied to a stream given by csp_set_stream.
                                     No counterpart in the reference. */
+#define CSP_FLAG_TENSOR_CORES 0x20 /* generic BCSR SpMM (csp_init_bcsr_kernels, nrhs a multiple of 32, blocks of
+                                    at most 8 rows x 4 columns) on the tensor cores: mma.sync m16n8k8 with TF32
+                                    operands split in high and low parts for FP32 accuracy.  No counterpart
+                                    in the reference. */
 
 /* Kernel choice for a CSR or COO sub-matrix (csr_meth_num / coo_meth_num; no
  * counterpart in the reference): x staged in shared memory by column panels of at
@@ -421,16 +425,20 @@ int csp_spmv_sbell(coo_matrix_if* coo, int ntimes, csp_report* report);
 /*   d_abar[s] = d_ybar[row(s)] * x[col(s)] for every stored slot s of the     */
 /*   forward parts, in launch order, each part in its own storage layout      */
 /*   (DIA/BDIA: diagonal-major slots; CSR/COO: entry order; ELL/SELL: their     */
-/*   slot order) -- the gradient of ybar^T (A x) with respect to the stored    */
-/*   values.  x is the handle's current vector.  All pointers are device       */
-/*   pointers; d_xbar or d_abar may be NULL to skip that output.  Value        */
-/*   gradients of block-format parts are not provided (CSP_EUNSUP).            */
+/*   slot order; BCSR/BELL/SBELL: their b4 data order) -- the gradient of      */
+/*   ybar^T (A x) with respect to the stored values.  A handle of              */
+/*   csp_init_bcsr_kernels (one right-hand side) takes CSP_FLAG_ADJOINT too:   */
+/*   its slots are the caller's generic BCSR data order, data[e * aligned + j] */
+/*   (element e of block j at row e / bw, column e % bw).  x is the handle's   */
+/*   current vector.  All pointers are device pointers; d_xbar or d_abar may   */
+/*   be NULL to skip that output.                                              */
 /* ------------------------------------------------------------------------ */
 int csp_spmv_adjoint(csp_handle* h, const float* d_ybar, float* d_xbar, float* d_abar);
 /* Number of stored slots, the length of d_abar. */
 int csp_adjoint_slots(csp_handle* h, size_t* nslots);
 /* Row and column of every slot (row -1 for slots outside the matrix: alignment
- * rows, out-of-range diagonal positions), into device arrays of nslots ints. */
+ * rows and blocks, out-of-range diagonal positions, the parts of a last block row
+ * or column past the matrix), into device arrays of nslots ints. */
 int csp_adjoint_pattern(csp_handle* h, int* d_rows, int* d_cols);
 
 /* ------------------------------------------------------------------------ */
@@ -524,17 +532,23 @@ int csp_batch_pattern(const csp_batch* b, int i, int* rows, int* cols);
 /* framework allocator that already owns the device, real-time loops where    */
 /* cudaMalloc/cudaFree (which may synchronize the device) are forbidden,      */
 /* embedders that pass only buffers they own.  Computes y += A*x for a COO    */
-/* matrix held by the caller in device memory (rows sorted, 16-byte aligned   */
-/* arrays), on `stream` (NULL = legacy default stream), allocating nothing:   */
-/* its scratch is a fixed 1 MiB array inside this library's device image,     */
-/* held by every GPU that loads the library until the process exits, which    */
-/* limits nnz to CSP_NOALLOC_MAX_NNZ (larger matrices: CSP_EINVAL).           */
+/* matrix held by the caller in device memory (16-byte aligned arrays), on    */
+/* `stream` (NULL = legacy default stream), allocating nothing: its scratch   */
+/* is a fixed 1 MiB array inside this library's device image, held by every   */
+/* GPU that loads the library until the process exits, which limits nnz to   */
+/* CSP_NOALLOC_MAX_NNZ (larger matrices: CSP_EINVAL).                         */
+/* Preconditions, not checked on the device (checking would need a pass and a */
+/* synchronization): rows sorted in nondecreasing order -- unsorted input     */
+/* gives an undefined result, though no access leaves the caller's arrays --  */
+/* and x and y distinct, non-overlapping arrays (d_x == d_y: CSP_EINVAL).     */
 /* The first call on each device looks the array's address up for that       */
-/* device, so make it before capturing the call into a CUDA graph.  All calls */
-/* on a device share the array: calls that overlap on the GPU (other streams, */
-/* other host threads) race and must be serialized by the caller.  Nothing in */
-/* the array needs clearing between calls: each call writes every slot it     */
-/* reads.  Out-of-range row or column ids are skipped, not dereferenced.      */
+/* device and keeps it, so make it before capturing the call into a CUDA      */
+/* graph; a cudaDeviceReset after that first call is not supported.  All     */
+/* calls on a device share the array: calls that overlap on the GPU (other   */
+/* streams, other host threads) race and must be serialized by the caller.    */
+/* Nothing in the array needs clearing between calls: each call writes every  */
+/* slot it reads.  Out-of-range row or column ids are skipped, not            */
+/* dereferenced.                                                              */
 /* ------------------------------------------------------------------------ */
 #define CSP_NOALLOC_MAX_NNZ       33554432   /* 2^25 entries                          */
 #define CSP_NOALLOC_SCRATCH_BYTES 1048576    /* 2 (row, partial) pairs per 512 entries */

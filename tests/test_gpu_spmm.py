@@ -114,3 +114,28 @@ def test_generic_bcsr_ragged(name, bs, k, bf16):
     hd.free()
     capi.lib().csp_free_bcsr_matrix(C.byref(b))
     _check_cols(case, Y, X, Y0, k, values=bf16_round(v) if bf16 else None)
+
+
+TENSOR_CASES = {**CASES, **RAGGED}
+
+
+@pytest.mark.parametrize("name,bs", [("block3", 3), ("block4", 4), ("zipf", 2), ("zipf", 1), ("ragged", 3),
+                                     ("ragged_long", 4), ("ragged", 2)])
+@pytest.mark.parametrize("k", [32, 64, 33])
+@pytest.mark.parametrize("bf16", [False, True])
+def test_generic_bcsr_spmm_tensor_cores(name, bs, k, bf16):
+    """CSP_FLAG_TENSOR_CORES: the mma.sync path for k a multiple of 32 (k = 33 keeps the
+    CUDA-core kernel), including empty and partial block rows and odd block counts."""
+    from clspmv_b200 import CSP_FLAG_TENSOR_CORES
+    case = TENSOR_CASES[name]
+    h, w, r, c, v = case
+    b = capi.bcsr_matrix()
+    assert capi.lib().csp_coo2bcsr(coo_of(case).ref(), C.byref(b), bs, bs, 32) == 0
+    X, Y0 = _xy(h, w, k, seed=11)
+    flags = CSP_FLAG_TENSOR_CORES | (CSP_FLAG_BF16 if bf16 else 0)
+    hd = Handle(None, X, Y0, flags=flags, nrhs=k, bcsr=b)
+    hd.do_spmv(1)
+    Y = hd.cpy_result_to_cpu()
+    hd.free()
+    capi.lib().csp_free_bcsr_matrix(C.byref(b))
+    _check_cols(case, Y, X, Y0, k, values=bf16_round(v) if bf16 else None)
