@@ -22,6 +22,7 @@ CSP_OK, CSP_EINVAL, CSP_ENOMEM, CSP_ECUDA, CSP_EFORMAT, CSP_ENODEV, CSP_EUNSUP, 
 CSP_FLAG_USE_TEX, CSP_FLAG_BF16, CSP_FLAG_GRAPH, CSP_FLAG_ADJOINT, CSP_FLAG_L2_PERSIST = 0x1, 0x2, 0x4, 0x8, 0x10
 CSP_FLAG_TENSOR_CORES = 0x20
 CSP_METH_XPANEL = 16
+CSP_METH_GENERIC_BCSR = 32
 CSP_ANALYZE_REFERENCE, CSP_ANALYZE_AUTOTUNE = 0, 1
 CSP_NOALLOC_MAX_NNZ = 33554432
 CSP_BFMT_AUTO = -1
@@ -197,6 +198,7 @@ def _declare(lib):
         "csp_bcsr2coo": (C.c_int, [P(bcsr_matrix), P(coo_matrix)]),
         "csp_coo2bell": (C.c_int, [P(coo_matrix), P(bell_matrix), C.c_uint, C.c_uint, C.c_int, C.c_int]),
         "csp_bell2coo": (C.c_int, [P(bell_matrix), P(coo_matrix)]),
+        "csp_rearrange_bell_4col": (C.c_int, [P(bell_matrix), C.c_int]),
         "csp_coo2b4csr": (C.c_int, [P(coo_matrix), P(b4csr_matrix), C.c_uint, C.c_uint, C.c_int]),
         "csp_coo2b4ell": (C.c_int, [P(coo_matrix), P(b4ell_matrix), C.c_uint, C.c_uint, C.c_int, C.c_int]),
         "csp_coo2sbell": (C.c_int, [P(coo_matrix), P(sbell_matrix), C.c_uint, C.c_uint, C.c_uint]),

@@ -26,7 +26,6 @@ namespace csp {
 
 namespace {
 
-struct Entry { int r, c; float v; };
 
 // Every stored slot of a b4 block layout (matrix_storage.h:2203 SBELL, :2010 BELL,
 // :1741 BCSR): f(i, row, col) with i the slot's index in the part's data array and
@@ -102,6 +101,25 @@ template <class F> void for_each_bcsr_slot(const b4csr_matrix_if& b, F f)
         if (!seen[i]) f(i, -1, -1);   // alignment slots past the last block
 }
 
+// Nonzeros of a generic BCSR (matrix_storage.h:1595 layout: element e of block j at
+// row brow(j) * bh + e / bw, column col[j] + e % bw).
+void gather_generic_bcsr(const bcsr_matrix_if& b, std::vector<Entry>& out)
+{
+    const int bw = (int)b.bcsr_bwidth, bh = (int)b.bcsr_bheight, al = b.bcsr_aligned_size;
+    for (int br = 0; br < b.bcsr_row_num; br++)
+        for (int j = b.bcsr_row_ptr[br]; j < b.bcsr_row_ptr[br + 1]; j++)
+            for (int q = 0; q < bh * bw; q++) {
+                const int r = br * bh + q / bw, c = b.bcsr_col_id[j] + q % bw;
+                const float v = b.bcsr_data[(size_t)q * al + j];
+                if (r < b.matinfo.height && c < b.matinfo.width && v != 0.0f) out.push_back(Entry{r, c, v});
+            }
+}
+
+const bcsr_matrix_if& generic_of(const cocktail_iif* mat)
+{
+    return *reinterpret_cast<const bcsr_matrix_if*>(&mat->bcsr);
+}
+
 // Nonzeros of the non-diagonal parts of `mat`, gathered from their host layouts.
 void gather_entries(const cocktail_iif* mat, bool include_diag, std::vector<Entry>& out)
 {
@@ -130,7 +148,8 @@ void gather_entries(const cocktail_iif* mat, bool include_diag, std::vector<Entr
     auto add_slot = [&](size_t i, int r, int c, const float* data) { if (r >= 0) add(r, c, data[i]); };
     if (mat->ifusesbell) for_each_sbell_slot(mat->sbell, [&](size_t i, int r, int c) { add_slot(i, r, c, mat->sbell.sbell_data); });
     if (mat->ifusebell) for_each_bell_slot(mat->bell, [&](size_t i, int r, int c) { add_slot(i, r, c, mat->bell.b4ell_data); });
-    if (mat->ifusebcsr) for_each_bcsr_slot(mat->bcsr, [&](size_t i, int r, int c) { add_slot(i, r, c, mat->bcsr.b4csr_data); });
+    if (mat->ifusebcsr && mat->bcsr_meth_num == CSP_METH_GENERIC_BCSR) gather_generic_bcsr(generic_of(mat), out);
+    else if (mat->ifusebcsr) for_each_bcsr_slot(mat->bcsr, [&](size_t i, int r, int c) { add_slot(i, r, c, mat->bcsr.b4csr_data); });
     if (mat->ifusesell) {
         const sell_matrix_if& s = mat->sell;
         const int H = (int)s.sell_slice_height;
@@ -200,50 +219,15 @@ int Engine::add_slot_list(Seg& s, const std::vector<int>& rows, const std::vecto
 // slot of the caller's BCSR layout (data[e * aligned + block], matrix_storage.h:1595),
 // element e of a block being row e / bw, column e % bw; alignment slots, and slots
 // of a partial last block row or column, get row -1.
-int Engine::build_adjoint_gbcsr(const bcsr_matrix_if& b)
+// The value-gradient segment of a generic BCSR part: every slot of the caller's layout.
+int Engine::gbcsr_segment(const bcsr_matrix_if& b, Seg& s)
 {
-    adjoint = true;
     const int bw = (int)b.bcsr_bwidth, bh = (int)b.bcsr_bheight, al = b.bcsr_aligned_size, nb = b.bcsr_block_num;
-    std::vector<Entry> e;
     std::vector<int> brow((size_t)std::max(nb, 1), -1);
     for (int br = 0; br < b.bcsr_row_num; br++)
-        for (int j = b.bcsr_row_ptr[br]; j < b.bcsr_row_ptr[br + 1]; j++) {
-            brow[j] = br;
-            for (int q = 0; q < bh * bw; q++) {
-                const int r = br * bh + q / bw, c = b.bcsr_col_id[j] + q % bw;
-                const float v = b.bcsr_data[(size_t)q * al + j];
-                if (r < height && c < width && v != 0.0f) e.push_back(Entry{r, c, v});
-            }
-        }
-    int rc = CSP_OK;
-    std::swap(width, height);
-    std::swap(parts, adj_parts);
-    if (!e.empty()) {
-        std::stable_sort(e.begin(), e.end(), [](const Entry& p, const Entry& q) { return p.c != q.c ? p.c < q.c : p.r < q.r; });
-        csr_matrix_if t;
-        csp_init_csr_matrix(&t);
-        std::vector<int> rp((size_t)height + 1, 0), col(e.size());
-        std::vector<float> val(e.size());
-        for (size_t i = 0; i < e.size(); i++) {
-            rp[(size_t)e[i].c + 1]++;
-            col[i] = e[i].r;
-            val[i] = e[i].v;
-        }
-        for (int i = 0; i < height; i++) rp[i + 1] += rp[i];
-        t.matinfo.width = width;
-        t.matinfo.height = height;
-        t.matinfo.nnz = (int)e.size();
-        t.csr_row_ptr = rp.data();
-        t.csr_col_id = col.data();
-        t.csr_data = val.data();
-        rc = add_csr(t, 2);
-    }
-    std::swap(parts, adj_parts);
-    std::swap(width, height);
-    if (rc) return rc;
-    Seg s;
-    s.offset = 0;
+        for (int j = b.bcsr_row_ptr[br]; j < b.bcsr_row_ptr[br + 1]; j++) brow[j] = br;
     int *d_brow = nullptr, *d_col = nullptr;
+    int rc;
     if ((rc = upload_int(&d_brow, brow.data(), (size_t)nb, std::max<size_t>(nb, 1))) ||
         (rc = upload_int(&d_col, b.bcsr_col_id, (size_t)nb, std::max<size_t>(nb, 1))))
         return rc;
@@ -254,9 +238,56 @@ int Engine::build_adjoint_gbcsr(const bcsr_matrix_if& b)
     s.p1 = nb;
     s.p2 = bh * 16 + bw;
     s.count = (size_t)al * bh * bw;
+    return CSP_OK;
+}
+
+// Adjoint of a generic BCSR handle (csp_init_bcsr_kernels with CSP_FLAG_ADJOINT): A^T
+// as one transposed CSR part of the blocks' nonzeros, and value gradients over every
+// slot of the caller's BCSR layout (data[e * aligned + block], matrix_storage.h:1595),
+// element e of a block being row e / bw, column e % bw; alignment slots, and slots
+// of a partial last block row or column, get row -1.
+int Engine::build_adjoint_gbcsr(const bcsr_matrix_if& b)
+{
+    adjoint = true;
+    std::vector<Entry> e;
+    gather_generic_bcsr(b, e);
+    int rc = add_transposed_csr(e);
+    if (rc) return rc;
+    Seg s;
+    s.offset = 0;
+    if ((rc = gbcsr_segment(b, s))) return rc;
     segs.push_back(s);
     abar_total = s.count;
     return CSP_OK;
+}
+
+// A^T of the given entries (of A) as one CSR part of adj_parts, the adaptive kernel.
+int Engine::add_transposed_csr(std::vector<Entry>& e)
+{
+    if (e.empty()) return CSP_OK;
+    std::swap(width, height);
+    std::swap(parts, adj_parts);
+    std::stable_sort(e.begin(), e.end(), [](const Entry& p, const Entry& q) { return p.c != q.c ? p.c < q.c : p.r < q.r; });
+    csr_matrix_if t;
+    csp_init_csr_matrix(&t);
+    std::vector<int> rp((size_t)height + 1, 0), col(e.size());
+    std::vector<float> val(e.size());
+    for (size_t i = 0; i < e.size(); i++) {
+        rp[(size_t)e[i].c + 1]++;
+        col[i] = e[i].r;
+        val[i] = e[i].v;
+    }
+    for (int i = 0; i < height; i++) rp[i + 1] += rp[i];
+    t.matinfo.width = width;
+    t.matinfo.height = height;
+    t.matinfo.nnz = (int)e.size();
+    t.csr_row_ptr = rp.data();
+    t.csr_col_id = col.data();
+    t.csr_data = val.data();
+    const int rc = add_csr(t, 2);
+    std::swap(parts, adj_parts);
+    std::swap(width, height);
+    return rc;
 }
 
 int Engine::build_adjoint(const cocktail_iif* mat)
@@ -295,36 +326,14 @@ int Engine::build_adjoint(const cocktail_iif* mat)
         std::vector<int> off(d.dia_offsets, d.dia_offsets + d.dia_num);
         rc = add_tdia(off, d.dia_data, d.dia_length_aligned, std::min(d.matinfo.height, d.dia_length_aligned), 1);
     }
-    if (!rc) {
-        std::vector<Entry> e;
-        gather_entries(mat, !square, e);
-        if (!e.empty()) {
-            std::stable_sort(e.begin(), e.end(), [](const Entry& a, const Entry& b) {
-                return a.c != b.c ? a.c < b.c : a.r < b.r;
-            });
-            // CSR of A^T: row = original column
-            csr_matrix_if t;
-            csp_init_csr_matrix(&t);
-            std::vector<int> rp((size_t)height + 1, 0), col(e.size());
-            std::vector<float> val(e.size());
-            for (size_t i = 0; i < e.size(); i++) {
-                rp[(size_t)e[i].c + 1]++;
-                col[i] = e[i].r;
-                val[i] = e[i].v;
-            }
-            for (int i = 0; i < height; i++) rp[i + 1] += rp[i];
-            t.matinfo.width = width;
-            t.matinfo.height = height;
-            t.matinfo.nnz = (int)e.size();
-            t.csr_row_ptr = rp.data();
-            t.csr_col_id = col.data();
-            t.csr_data = val.data();
-            rc = add_csr(t, 2);
-        }
-    }
     std::swap(parts, adj_parts);
     std::swap(width, height);
     if (rc) return rc;
+    {
+        std::vector<Entry> e;
+        gather_entries(mat, !square, e);
+        if ((rc = add_transposed_csr(e))) return rc;
+    }
 
     // --- value-gradient segments over the forward parts, in launch order ---
     abar_total = 0;
@@ -421,6 +430,9 @@ int Engine::build_adjoint(const cocktail_iif* mat)
             s.p1 = mat->sell.sell_slice_num;
             s.p2 = p.m;
             s.count = (size_t)mat->sell.sell_slice_ptr[mat->sell.sell_slice_num];
+            break;
+        case PART_GBCSR:
+            if ((rc = gbcsr_segment(generic_of(mat), s))) return rc;
             break;
         case PART_SBELL:
         case PART_BELL:

@@ -178,7 +178,8 @@ int build_sell_split(const Coo& a, int sh, double q, int csr_meth, cocktail_iif*
 
 // Builds the candidate named `name` into c (fresh, zeroed).  Names: csr<m>, coo,
 // ell, sell<sh>, dia<m>, bdia<m>, bcsr<bh>x<bw>m<m>, bell<bh>x<bw>, sbell<bh>x<bw>,
-// ell<k>+csr<m>, sellq<sh>+csr<m> (m = the overflow CSR part's kernel).  csr16 is the
+// ell<k>+csr<m>, sellq<sh>+csr<m> (m = the overflow CSR part's kernel), gbcsr<bh>x<bw>
+// (generic BCSR in the cocktail's bcsr member, CSP_METH_GENERIC_BCSR).  csr16 is the
 // x-panel kernel (CSP_METH_XPANEL).
 int build(const Coo& a, const std::string& name, cocktail_iif* c)
 {
@@ -188,6 +189,11 @@ int build(const Coo& a, const std::string& name, cocktail_iif* c)
     int x = 0, y = 0, z = 0;
     if (sscanf(name.c_str(), "ell%d+csr%d", &x, &y) == 2) return build_ell_split(a, x, y, c);
     if (sscanf(name.c_str(), "sellq%d+csr%d", &x, &y) == 2) return build_sell_split(a, x, 0.75, y, c);
+    if (sscanf(name.c_str(), "gbcsr%dx%d", &x, &y) == 2) {
+        c->ifusebcsr = true;
+        c->bcsr_meth_num = CSP_METH_GENERIC_BCSR;
+        return csp_coo2bcsr(m, reinterpret_cast<bcsr_matrix_if*>(&c->bcsr), (unsigned)y, (unsigned)x, 32);
+    }
     if (sscanf(name.c_str(), "bcsr%dx%dm%d", &x, &y, &z) == 3) {
         c->ifusebcsr = true;
         c->bcsr_meth_num = z;
@@ -269,7 +275,23 @@ std::vector<std::string> candidates(const Coo& a)
     const int h = m->matinfo.height, w = m->matinfo.width;
     const long long nnz = m->matinfo.nnz;
     const double mean = h ? (double)nnz / h : 0.0;
+    // generic BCSR block shapes (any alignment of the block grid the b4 formats need)
+    std::vector<std::string> blocks;
+    double best_fill = 0.0;
+    for (int b : {2, 3, 4, 6, 8}) {
+        const double fill = sampled_fill(a, b, b);
+        if (fill < 0.5) continue;
+        best_fill = std::max(best_fill, fill);
+        blocks.push_back("gbcsr" + std::to_string(b) + "x" + std::to_string(b));
+    }
+    // a matrix made of dense blocks: the block layouts and plain CSR (the baseline) only;
+    // flat formats would store every block entry with its own column id
+    if (best_fill >= 0.95) {
+        blocks.insert(blocks.begin(), "csr2");
+        return blocks;
+    }
     std::vector<std::string> c = {"csr2", "coo", "csr16"};
+    c.insert(c.end(), blocks.begin(), blocks.end());
     if (mean >= 12.0) c.push_back("csr0");
     if (a.maxlen <= 64 && mean >= 2.0) c.push_back("csr3");
     // ELL / SELL when the padding stays below 1.5x / 2x of the nonzeros

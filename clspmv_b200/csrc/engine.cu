@@ -1065,10 +1065,17 @@ int Engine::init(const cocktail_iif* mat, const float* vec, const float* res, in
     if (!mat) return set_error(CSP_EINVAL, "null cocktail");
     int rc = init_common(mat->mat_width, mat->mat_height, mat->mat_nnz, vec, res, flags, k);
     if (rc) return rc;
+    static_assert(sizeof(bcsr_matrix_if) == sizeof(b4csr_matrix_if) &&
+                      offsetof(bcsr_matrix_if, bcsr_row_ptr) == offsetof(b4csr_matrix_if, b4csr_row_ptr) &&
+                      offsetof(bcsr_matrix_if, bcsr_data) == offsetof(b4csr_matrix_if, b4csr_data),
+                  "generic and b4 BCSR structs share one layout");
+    const bool generic_bcsr = mat->ifusebcsr && mat->bcsr_meth_num == CSP_METH_GENERIC_BCSR;
     if (nrhs > 1) {
-        if (mat->ifusebdia || mat->ifusedia || mat->ifusesbell || mat->ifusebell || mat->ifusebcsr || mat->ifusesell ||
-            mat->ifuseell || mat->ifusecoo)
-            return set_error(CSP_EUNSUP, "several right-hand sides run on CSR parts (and csp_init_bcsr_kernels)");
+        if (mat->ifusebdia || mat->ifusedia || mat->ifusesbell || mat->ifusebell || (mat->ifusebcsr && !generic_bcsr) ||
+            mat->ifusesell || mat->ifuseell || mat->ifusecoo)
+            return set_error(CSP_EUNSUP, "several right-hand sides run on CSR and generic BCSR parts (and csp_init_bcsr_kernels)");
+        if (generic_bcsr && mat->bcsr.b4csr_bwidth * mat->bcsr.b4csr_bheight > 36)
+            return set_error(CSP_EUNSUP, "several right-hand sides need blocks of <= 36 elements");
         if (flags & CSP_FLAG_ADJOINT) return set_error(CSP_EUNSUP, "adjoint with several right-hand sides");
     }
     // parts, in the reference's launch order
@@ -1076,7 +1083,12 @@ int Engine::init(const cocktail_iif* mat, const float* vec, const float* res, in
     if (mat->ifusedia && (rc = add_dia(mat->dia, mat->dia_meth_num))) return rc;
     if (mat->ifusesbell && (rc = add_sbell(mat->sbell, mat->sbell_meth_num))) return rc;
     if (mat->ifusebell && (rc = add_bell(mat->bell, mat->bell_meth_num))) return rc;
-    if (mat->ifusebcsr && (rc = add_bcsr(mat->bcsr, mat->bcsr_meth_num))) return rc;
+    if (generic_bcsr) {
+        // the member holds a generic BCSR (same fields as the b4 struct, see CSP_METH_GENERIC_BCSR)
+        if ((rc = add_generic_bcsr(*reinterpret_cast<const bcsr_matrix_if*>(&mat->bcsr), 0))) return rc;
+    } else if (mat->ifusebcsr && (rc = add_bcsr(mat->bcsr, mat->bcsr_meth_num))) {
+        return rc;
+    }
     if (mat->ifusesell && (rc = add_sell(mat->sell, mat->sell_meth_num))) return rc;
     if (mat->ifuseell && (rc = add_ell(mat->ell, mat->ell_meth_num))) return rc;
     if (mat->ifusecsr && (rc = add_csr(mat->csr, mat->csr_meth_num))) return rc;

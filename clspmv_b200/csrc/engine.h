@@ -50,6 +50,9 @@ struct Part {
     bool from_csr = false;            // adjoint: value-gradient order follows the CSR part
 };
 
+// One matrix entry (row, column, value), as the adjoint builders gather them.
+struct Entry { int r, c; float v; };
+
 enum SegKind { SEG_NONE, SEG_DIA, SEG_LIST, SEG_ELL, SEG_SELL, SEG_GBCSR };
 
 // One forward part's share of the value-gradient array (adjoint).
@@ -100,6 +103,8 @@ struct Engine {
     int enqueue_parts(const std::vector<Part>& ps, const float* x, float* y, int n, cudaStream_t st);
     int build_adjoint(const cocktail_iif* mat);
     int build_adjoint_gbcsr(const bcsr_matrix_if& b);
+    int gbcsr_segment(const bcsr_matrix_if& b, Seg& s);
+    int add_transposed_csr(std::vector<Entry>& e);
     int add_slot_list(Seg& s, const std::vector<int>& rows, const std::vector<int>& cols);
     int launch_abar(const float* ybar, float* abar, int* prow, int* pcol, cudaStream_t st);
     int launches_per_spmv() const;

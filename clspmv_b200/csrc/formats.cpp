@@ -805,6 +805,41 @@ int csp_coo2sbell(coo_matrix_if* s, sbell_matrix_if* d, unsigned bw, unsigned bh
     return write_sbell(b, bw, bh, sh, width, d);
 }
 
+// util.cpp:273 rearrange_bell_4col: a generic BELL whose block width is a multiple of 4
+// rewritten in place into the float4 layout of the b4 kernels.  Element (h, w) of the
+// block in ELL slot i of block row j moves from
+//   data[i * hal * bw * bh + h * hal * bw + w * hal + j]            (hal = bell_height_aligned)
+// to
+//   data[i * f4 * w4 * bh + h * f4 + (w / 4) * f4 * bh + 4 * j + w % 4]
+// with f4 = bell_float4_aligned = align(4 * row_num, alignment) and w4 = bw / 4; the
+// column ids become float4 ids (divided by 4).  The slots between 4 * row_num and f4
+// are zero here; the reference leaves them uninitialized.
+int csp_rearrange_bell_4col(bell_matrix_if* m, int alignment)
+{
+    if (!m || alignment <= 0) return set_error(CSP_EINVAL, "rearrange_bell_4col: bad argument");
+    const int bw = (int)m->bell_bwidth, bh = (int)m->bell_bheight;
+    if (bw <= 0 || bw % 4 != 0) return set_error(CSP_EINVAL, "rearrange_bell_4col: block width %d is not a multiple of 4", bw);
+    const int ellnum = m->bell_block_num, rows = m->bell_row_num, hal = m->bell_height_aligned;
+    const int w4 = bw / 4;
+    const int f4 = csp_aligned_length(4 * rows, alignment);
+    const size_t n = (size_t)f4 * bh * w4 * ellnum;
+    float* nd = xcalloc<float>(std::max<size_t>(n, 1));
+    if (!nd) return set_error(CSP_ENOMEM, "rearrange_bell_4col");
+    const size_t col_old = (size_t)hal * bw * bh, h_old = (size_t)hal * bw;
+    const size_t col_new = (size_t)f4 * w4 * bh, w4_new = (size_t)f4 * bh;
+    for (int i = 0; i < ellnum; i++)
+        for (int h = 0; h < bh; h++)
+            for (int w = 0; w < bw; w++)
+                for (int j = 0; j < rows; j++)
+                    nd[i * col_new + (size_t)h * f4 + (size_t)(w / 4) * w4_new + (size_t)j * 4 + w % 4] =
+                        m->bell_data[i * col_old + (size_t)h * h_old + (size_t)w * hal + j];
+    free(m->bell_data);
+    m->bell_data = nd;
+    m->bell_float4_aligned = f4;
+    for (size_t i = 0; i < (size_t)hal * ellnum; i++) m->bell_col_id[i] /= 4;
+    return CSP_OK;
+}
+
 // util.cpp:31 pad_csr: every row padded to a multiple of `alignment` with the row's last
 // column id and value 0.  (An empty first row reads before the array in the reference;
 // here padding of an empty row is simply empty, which is what findPaddedSize(0) asks.)

@@ -241,13 +241,6 @@ namespace dev {
 // so they do not perturb the large one's rounding (the dropped al*xl is below 2^-22 of
 // |a x|).  BF16 values are exact in TF32 (al = 0): two MMAs.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t tf32_rna(float f)
-{
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(f));
-    return r;
-}
-
 __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
                                          uint32_t b1)
 {
@@ -257,10 +250,13 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], uint32_t a0, uint32_t a1
                  : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-// high and low TF32 parts of v (the low part as raw FP32 bits: the MMA reads its top 19)
+// High and low TF32 parts of v: hi = v rounded to nearest (ties away from zero) at
+// TF32's 10 fraction bits -- half a TF32 ulp (bit 12) added to the magnitude bits, the
+// 13 low bits cleared -- and the exact remainder lo = v - hi, passed as raw FP32 bits
+// (the MMA reads its top 19).  Finite |v| below 2^128 (1 - 2^-11) only.
 __device__ __forceinline__ void tf32_split(float v, uint32_t& hi, uint32_t& lo)
 {
-    hi = tf32_rna(v);
+    hi = (__float_as_uint(v) + 0x1000u) & 0xffffe000u;
     lo = __float_as_uint(v - __uint_as_float(hi));
 }
 

@@ -268,6 +268,10 @@ int csp_coo2bcsr(coo_matrix_if* src, bcsr_matrix_if* dst, unsigned int bwidth, u
 int csp_bcsr2coo(const bcsr_matrix_if* src, coo_matrix_if* dst);     /* matrix_storage.h:1546 */
 int csp_coo2bell(coo_matrix_if* src, bell_matrix_if* dst, unsigned int bwidth, unsigned int bheight, int alignment, int ellnum); /* :1941 */
 int csp_bell2coo(const bell_matrix_if* src, coo_matrix_if* dst);     /* matrix_storage.h:1901 */
+/* util.cpp:273 rearrange_bell_4col: a generic BELL with bwidth % 4 == 0 rewritten in place
+ * into the b4 float4 layout (bell_float4_aligned = align(4 * row_num, alignment), column
+ * ids divided by 4).  Alignment slots are zero (the reference leaves them unset). */
+int csp_rearrange_bell_4col(bell_matrix_if* mat, int alignment);
 int csp_coo2b4csr(coo_matrix_if* src, b4csr_matrix_if* dst, unsigned int bwidth, unsigned int bheight, int alignment); /* :1741; CSP_EFORMAT above MAX_MEM_OBJ */
 int csp_coo2b4ell(coo_matrix_if* src, b4ell_matrix_if* dst, unsigned int bwidth, unsigned int bheight, int alignment, int ellnum); /* :2010 */
 int csp_coo2sbell(coo_matrix_if* src, sbell_matrix_if* dst, unsigned int bwidth, unsigned int bheight, unsigned int sliceheight); /* :2203 */
@@ -338,6 +342,16 @@ typedef struct csp_handle csp_handle;
  * whose column indices have no locality (random graphs), where gathering x from
  * global memory is bound by L2 request throughput.  One right-hand side only. */
 #define CSP_METH_XPANEL    16
+
+/* bcsr_meth_num value marking the cocktail's `bcsr` member as a generic BCSR
+ * (matrix_storage.h:1595 coo2bcsr layout: column ids of the block's first column,
+ * data[e * aligned + block]) of one of the block shapes csp_init_bcsr_kernels takes,
+ * instead of the b4 layout.  bcsr_matrix_if and b4csr_matrix_if have the same fields
+ * in the same order, so the generic matrix is stored in the member as is and
+ * csp_free_cocktail frees it.  The autotuner (CSP_ANALYZE_AUTOTUNE) uses it for block
+ * shapes the b4 formats cannot hold, such as 3x3.  Such a part also takes several
+ * right-hand sides.  No counterpart in the reference. */
+#define CSP_METH_GENERIC_BCSR 32
 
 /* Upload every used sub-matrix of `mat`, x = vec (length mat_width) and
  * res (length mat_height; may be NULL for zeros), and select one kernel per

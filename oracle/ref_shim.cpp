@@ -13,7 +13,7 @@
 //       coo2sbell :2203, dia2coo :826, bdia2coo :1137,
 //       ell2coo :1310, bcsr2coo :1546, bell2coo :1901
 //   include/spmv_serial.h    : {dia,bdia,ell,sell,sbell,coo,csr,bcsr,bell}_spmv :12-279
-//   src/util.cpp             : pad_csr :31
+//   src/util.cpp             : pad_csr :31, rearrange_bell_4col :273
 //   src/analyze.cpp          : analyze_matrix :3704
 //   src/fileio.cpp           : ReadMMF :10
 // csr2coo (matrix_storage.h:1239) is not wrapped: instantiating it fails to compile
@@ -50,6 +50,7 @@ int ref_coo2b4csr(COO* s, b4csr_matrix<int, float>* d, unsigned int bw, unsigned
 int ref_coo2b4ell(COO* s, b4ell_matrix<int, float>* d, unsigned int bw, unsigned int bh, int alignment, int ellnum) { return coo2b4ell<int, float>(s, d, bw, bh, alignment, ellnum) ? 1 : 0; }
 int ref_coo2sbell(COO* s, sbell_matrix<int, float>* d, unsigned int bw, unsigned int bh, unsigned int sh) { return coo2sbell<int, float>(s, d, bw, bh, sh) ? 1 : 0; }
 void ref_pad_csr(CSR* s, CSR* d, int alignment) { pad_csr(s, d, alignment); }
+void ref_rearrange_bell_4col(bell_matrix<int, float>* m, int alignment) { rearrange_bell_4col(m, alignment); }
 
 void ref_dia_spmv(dia_matrix<int, int, float>* m, float* v, float* r, int n) { dia_spmv<int, int, float>(m, v, r, n); }
 void ref_bdia_spmv(bdia_matrix<int, int, float>* m, float* v, float* r, int n) { bdia_spmv<int, int, float>(m, v, r, n); }

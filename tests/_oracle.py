@@ -62,6 +62,7 @@ def ref_lib():
             "ref_coo2b4ell": [P(capi.coo_matrix), P(capi.b4ell_matrix), C.c_uint, C.c_uint, C.c_int, C.c_int],
             "ref_coo2sbell": [P(capi.coo_matrix), P(capi.sbell_matrix), C.c_uint, C.c_uint, C.c_uint],
             "ref_pad_csr": [P(capi.csr_matrix), P(capi.csr_matrix), C.c_int],
+            "ref_rearrange_bell_4col": [P(capi.bell_matrix), C.c_int],
             "ref_dia_spmv": [P(capi.dia_matrix), FP, FP, C.c_int],
             "ref_bdia_spmv": [P(capi.bdia_matrix), FP, FP, C.c_int],
             "ref_ell_spmv": [P(capi.ell_matrix), FP, FP, C.c_int],

@@ -144,3 +144,36 @@ def test_invalid_input_is_an_error_not_a_crash(L):
     e2 = capi.ell_matrix()
     two = COO(2, 4, [0, 0, 1], [0, 1, 2], [1, 2, 3])
     assert L.csp_coo2ell(two.ref(), C.byref(e2), 32, 1) == capi.CSP_EINVAL   # ellnum below the longest row
+
+
+@pytest.mark.parametrize("name", ["laplacian32", "random_irregular", "block3_small", "stencil6"])
+@pytest.mark.parametrize("shape", [(4, 1), (4, 2), (8, 2), (8, 4)], ids=lambda s: f"{s[0]}x{s[1]}")
+@pytest.mark.parametrize("alignment", [32, 7])
+def test_rearrange_bell_4col_bytes(L, ref, name, shape, alignment):
+    """util.cpp:273 rearrange_bell_4col on coo2bell output: float4 data layout and /4
+    column ids byte-identical to the reference's, except the alignment slots between
+    4 * row_num and float4_aligned, which the reference leaves uninitialized (malloc) and
+    this library zeroes."""
+    bw, bh = shape
+    a, b = _coo(CASES[name]), _coo(CASES[name])
+    sa, sb = capi.bell_matrix(), capi.bell_matrix()
+    assert L.csp_coo2bell(a.ref(), C.byref(sa), bw, bh, 32, 0) == 0
+    ref.ref_coo2bell(b.ref(), C.byref(sb), bw, bh, 32, 0)
+    assert L.csp_rearrange_bell_4col(C.byref(sa), alignment) == 0
+    ref.ref_rearrange_bell_4col(C.byref(sb), alignment)
+    for s in (sa, sb):
+        assert s.bell_float4_aligned == -(-4 * s.bell_row_num // alignment) * alignment
+    f4, rows, ell, w4 = sa.bell_float4_aligned, sa.bell_row_num, sa.bell_block_num, bw // 4
+    ncol = sa.bell_height_aligned * ell
+    ca = np.ctypeslib.as_array(sa.bell_col_id, shape=(max(ncol, 1),))[:ncol]
+    cb = np.ctypeslib.as_array(sb.bell_col_id, shape=(max(ncol, 1),))[:ncol]
+    assert np.array_equal(ca, cb)
+    n = f4 * bh * w4 * ell
+    da = np.ctypeslib.as_array(sa.bell_data, shape=(max(n, 1),))[:n].reshape(ell, w4, bh, f4)
+    db = np.ctypeslib.as_array(sb.bell_data, shape=(max(n, 1),))[:n].reshape(ell, w4, bh, f4)
+    defined = np.arange(f4) < 4 * rows
+    assert da[..., defined].tobytes() == db[..., defined].tobytes()
+    assert np.all(da[..., ~defined] == 0)
+    bad = capi.bell_matrix()
+    bad.bell_bwidth = 3
+    assert L.csp_rearrange_bell_4col(C.byref(bad), 32) == capi.CSP_EINVAL
