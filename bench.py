@@ -686,6 +686,7 @@ def run_single(dev, name, args, with_cpu: bool, steps: int, warmup: int):
     best = Handle(mat, x, y0, flags)
     partition = mat.choice
     out["setup_s"] = time.perf_counter() - t0
+    out["analyzer_s"] = reference_tables_analysis_s(mats[0])
     best.set_stream(dev.sp)
     step = lambda: best.do_spmv(1)  # noqa: E731
     times = dev.time(step, steps, warmup, l2_resident)
@@ -805,11 +806,29 @@ def run_single(dev, name, args, with_cpu: bool, steps: int, warmup: int):
     return out
 
 
+def reference_tables_analysis_s(case):
+    """Wall seconds of the reference-table partitioner (csp_analyze_matrix,
+    CSP_ANALYZE_REFERENCE) on this library's B200 calibration tables, with its counting
+    passes on the device (CSP_ANALYZE_ON_DEVICE): the one-time setup a caller of the
+    reference's analyze_matrix pays."""
+    from clspmv_b200 import COO, capi
+    tables = os.path.join(ROOT, "clspmv_b200", "tables_b200")
+    a = COO(*case)
+    mat = capi.cocktail()
+    opts = capi.csp_analyze_opts(capi.CSP_ANALYZE_REFERENCE, tables.encode(), 0, None, capi.CSP_ANALYZE_ON_DEVICE)
+    t0 = time.perf_counter()
+    rc = capi.lib().csp_analyze_matrix(a.ref(), C.byref(mat), C.byref(opts))
+    dt = time.perf_counter() - t0
+    capi.lib().csp_free_cocktail(C.byref(mat))
+    return dt if rc == 0 else None
+
+
 def summarize_leg(res, peak):
     """A config.legs entry from a run_single/run_batch result."""
     leg = {"workload": res["desc"], "nnz": res["nnz"], "partition": res["partition"], "ms": res["ms_step"],
            "gb_s": gbs(res["bytes"], res["ms_step"]), "frac": gbs(res["bytes"], res["ms_step"]) / peak,
-           "algorithmic_bytes": res["bytes"], "setup_s": res["setup_s"], "errors": res["errors"],
+           "algorithmic_bytes": res["bytes"], "setup_s": res["setup_s"],
+           "reference_tables_analysis_s": res.get("analyzer_s"), "errors": res["errors"],
            "plain_csr": res["plain"], "speedup_vs_plain_csr": res["plain"]["ms"] / res["ms_step"]}
     if "l2" in res:
         leg["l2"] = res["l2"]

@@ -23,6 +23,7 @@ CSP_FLAG_USE_TEX, CSP_FLAG_BF16, CSP_FLAG_GRAPH, CSP_FLAG_ADJOINT, CSP_FLAG_L2_P
 CSP_FLAG_TENSOR_CORES = 0x20
 CSP_METH_XPANEL = 16
 CSP_METH_GENERIC_BCSR = 32
+CSP_ANALYZE_ON_DEVICE = 0x100
 CSP_ANALYZE_REFERENCE, CSP_ANALYZE_AUTOTUNE = 0, 1
 CSP_NOALLOC_MAX_NNZ = 33554432
 CSP_BFMT_AUTO = -1

@@ -19,6 +19,7 @@
 // autotuner (autotune.cu), which times candidate partitions on the GPU.  Tables
 // measured on the B200 by csp_benchmark_tables (calibrate.cu) can still drive the
 // reference partitioner through CSP_ANALYZE_REFERENCE and a table path.
+#include <cuda_runtime.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -313,12 +314,14 @@ static T* dup(const vector<T>& v)
 
 class Analyzer {
   public:
-    Analyzer(const Tables& t, cocktail_iif& out) : T(t), mat(out) {}
+    Analyzer(const Tables& t, cocktail_iif& out, bool on_device = false) : T(t), mat(out), on_device(on_device) {}
     void run(Mat& coo);
+    int device_rc = CSP_OK;   // first error of a device counting pass (CSP_ANALYZE_ON_DEVICE)
 
   private:
     const Tables& T;
     cocktail_iif& mat;
+    bool on_device;
     Info info;
 
     double overhead(int groupnum, int threadnum) const;
@@ -481,9 +484,13 @@ bool Analyzer::extract_dia(const Mat& m, Mat& rem)
     if (least > m.h) return false;
     const int threshold = m.h - least;
     vector<int> count((size_t)2 * threshold + 1, 0);
-    for (int i = 0; i < m.nnz(); i++) {
-        const int o = m.c[i] - m.r[i] + threshold;
-        if (o >= 0 && o < (int)count.size()) count[o]++;
+    if (on_device && !device_rc) {
+        device_rc = device_count_dia(m.r.data(), m.c.data(), m.nnz(), threshold, count);
+    } else {
+        for (int i = 0; i < m.nnz(); i++) {
+            const int o = m.c[i] - m.r[i] + threshold;
+            if (o >= 0 && o < (int)count.size()) count[o]++;
+        }
     }
     vector<pair<int, int>> valid;
     for (int i = 0; i < (int)count.size(); i++)
@@ -713,7 +720,22 @@ bool Analyzer::extract_block(const Mat& m, Mat& rem)
         if (threshold[i] > kBh[i] * kBw[i] - 1) threshold[i] = kBh[i] * kBw[i] - 1;
     }
     vector<vector<BlockInfo>> bc;
-    count_blocks(m, rp, threshold, bc);
+    if (on_device && !device_rc) {
+        vector<vector<BlockCounts>> dc;
+        device_rc = device_count_blocks(rp.data(), m.c.data(), m.h, m.nnz(), kBh, kBw, threshold.data(), 8, dc);
+        bc.assign(8, vector<BlockInfo>());
+        for (int s = 0; s < 8 && !device_rc; s++) {
+            bc[s].resize(dc[s].size());
+            for (size_t j = 0; j < dc[s].size(); j++) {
+                bc[s][j].partial_blocks = dc[s][j].partial_blocks;
+                bc[s][j].partial_nnz = dc[s][j].partial_nnz;
+                bc[s][j].full_blocks = dc[s][j].full_blocks;
+                bc[s][j].full_nnz = dc[s][j].full_nnz;
+            }
+        }
+    } else {
+        count_blocks(m, rp, threshold, bc);
+    }
     vector<double> block_over(8, 0.0f);
     for (int i = 0; i < 8; i++) {
         block_over[i] = overhead(m.h / (kBh[i] * kSellGroup), kSellGroup);
@@ -1323,7 +1345,17 @@ extern "C" int csp_analyze_matrix(coo_matrix_if* coo, cocktail_iif* mat, const c
     m.r.assign(coo->coo_row_id, coo->coo_row_id + coo->matinfo.nnz);
     m.c.assign(coo->coo_col_id, coo->coo_col_id + coo->matinfo.nnz);
     m.v.assign(coo->coo_data, coo->coo_data + coo->matinfo.nnz);
-    ana::Analyzer a(t, *mat);
+    const bool on_device = opts && (opts->flags & CSP_ANALYZE_ON_DEVICE);
+    if (on_device) {
+        int ndev = 0;
+        if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+            return set_error(CSP_ENODEV, "CSP_ANALYZE_ON_DEVICE needs a CUDA device");
+    }
+    ana::Analyzer a(t, *mat, on_device);
     a.run(m);
+    if (a.device_rc) {
+        csp_free_cocktail(mat);
+        return a.device_rc;
+    }
     return CSP_OK;
 }

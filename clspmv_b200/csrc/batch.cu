@@ -34,7 +34,7 @@ namespace {
         if (_e != cudaSuccess) return cuda_error(_e, #call);        \
     } while (0)
 
-constexpr int kItemSlots = 4096;   // target stored slots per work item
+constexpr int kItemSlots = 2048;   // target stored slots per (warp) work item
 
 inline long long pad_ll(long long v, long long a) { return (v + a - 1) / a * a; }
 
@@ -245,6 +245,41 @@ void cut_items(HPart& p, int nvb, const std::vector<long long>& vb_slots)
     }
 }
 
+// CSR work blocks of one warp: runs of whole rows with at most dev::kWarpNnz entries
+// and dev::kWarpRows rows {first row, rows, first entry, end entry}, or the chunks of a
+// row longer than kWarpNnz {chunk, -(long row + 1), first entry, end entry} with the
+// long row {row, first partial slot, chunks, -}.
+void make_warp_blocks(const std::vector<int>& rp, int m, std::vector<int4>& blocks, std::vector<int4>& longs, int& nslots)
+{
+    blocks.clear();
+    longs.clear();
+    nslots = 0;
+    int r = 0;
+    while (r < m) {
+        const int len = rp[r + 1] - rp[r];
+        if (len > dev::kWarpNnz) {
+            const int lid = (int)longs.size();
+            const int nch = (len + dev::kWarpNnz - 1) / dev::kWarpNnz;
+            longs.push_back(make_int4(r, nslots, nch, 0));
+            for (int k = 0; k < nch; k++)
+                blocks.push_back(make_int4(k, -(lid + 1), rp[r] + k * dev::kWarpNnz,
+                                           std::min(rp[r] + (k + 1) * dev::kWarpNnz, rp[r + 1])));
+            nslots += nch;
+            r++;
+            continue;
+        }
+        const int start = r;
+        long long acc = 0;
+        while (r < m && r - start < dev::kWarpRows) {
+            const int l = rp[r + 1] - rp[r];
+            if (l > dev::kWarpNnz || acc + l > dev::kWarpNnz) break;
+            acc += l;
+            r++;
+        }
+        blocks.push_back(make_int4(start, r - start, rp[start], rp[r]));
+    }
+}
+
 void build_csr(const HCsr& c, HPart& p)
 {
     const int nnz = c.rp[c.m];
@@ -256,7 +291,7 @@ void build_csr(const HCsr& c, HPart& p)
     p.i1.resize((size_t)pad_ll(nnz, 4) + 4, 0);
     p.v = c.val;
     p.v.resize(p.i1.size(), 0.0f);
-    make_adaptive_blocks(c.rp.data(), c.m, p.blocks, p.longs, p.npartial);
+    make_warp_blocks(c.rp, c.m, p.blocks, p.longs, p.npartial);
     p.slots = nnz;
     p.ranges.clear();
     for (int b = 0; b < (int)p.blocks.size(); b++) p.ranges.push_back(range_item(b, b + 1, p.blocks[b]));
@@ -288,10 +323,13 @@ void build_sell(const HCsr& c, int H, HPart& p)
             p.v[q] = c.val[j];
         }
     }
-    const int nvb = (m + dev::kBatchThreads - 1) / dev::kBatchThreads;
-    const int spv = dev::kBatchThreads / H;   // slices per virtual block
+    // virtual blocks of 32 rows (a lane per row), inside one slice (H is 32 or 128)
+    const int nvb = (m + dev::kBatchSellRows - 1) / dev::kBatchSellRows;
     std::vector<long long> vs((size_t)nvb);
-    for (int vb = 0; vb < nvb; vb++) vs[vb] = p.i0[std::min(S, (vb + 1) * spv)] - p.i0[vb * spv];
+    for (int vb = 0; vb < nvb; vb++) {
+        const int s = vb * dev::kBatchSellRows / H;
+        vs[vb] = (long long)(p.i0[s + 1] - p.i0[s]) / H * dev::kBatchSellRows;
+    }
     cut_items(p, nvb, vs);
 }
 
@@ -316,7 +354,7 @@ void build_dia(const HCsr& c, HPart& p)
             const int d = (int)(std::lower_bound(offs.begin(), offs.end(), c.col[j] - r) - offs.begin());
             p.v[(size_t)d * p.stride + r] += c.val[j];   // duplicates share a slot
         }
-    const int rows_per_vb = dev::kBatchThreads * dev::kBatchDiaRows;
+    const int rows_per_vb = dev::kBatchDiaRows;
     const int nvb = (m + rows_per_vb - 1) / rows_per_vb;
     cut_items(p, nvb, std::vector<long long>((size_t)nvb, (long long)rows_per_vb * std::max(p.k, 1)));
 }
@@ -357,7 +395,7 @@ void build_bcsr(const HCsr& c, int B, HPart& p)
             p.v[(size_t)q * al + blk] += c.val[j];
         }
     }
-    const int brpv = dev::kBatchThreads / dev::kBatchBcsrLanes;   // block rows per virtual block
+    const int brpv = dev::kBatchBcsrRows;   // block rows per virtual block
     const int nvb = (nbr + brpv - 1) / brpv;
     std::vector<long long> vs((size_t)nvb);
     for (int vb = 0; vb < nvb; vb++)
@@ -476,17 +514,19 @@ int occupancy_grid(bool bf16, int nitems)
     else
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dev::batch_kernel<float>, dev::kBatchThreads, 0);
     const int g = std::max(1, sms) * std::max(1, per_sm);
-    return std::max(1, std::min(g, nitems));
+    return std::max(1, std::min(g, (nitems + dev::kBatchWarps - 1) / dev::kBatchWarps));
 }
 
-int launch_batch(bool bf16, const dev::BatchPart* parts, const dev::BatchItem* items, int nitems,
+// One launch over `nitems` items: the item counter zeroed on the stream, then the kernel.
+int launch_batch(bool bf16, const dev::BatchPart* parts, const dev::BatchItem* items, int nitems, int* counter,
                  unsigned long long* cycles, int grid, cudaStream_t st)
 {
     if (nitems <= 0) return CSP_OK;
+    BCUDA(cudaMemsetAsync(counter, 0, sizeof(int), st));
     if (bf16)
-        dev::batch_kernel<__nv_bfloat16><<<grid, dev::kBatchThreads, 0, st>>>(parts, items, nitems, cycles);
+        dev::batch_kernel<__nv_bfloat16><<<grid, dev::kBatchThreads, 0, st>>>(parts, items, nitems, counter, cycles);
     else
-        dev::batch_kernel<float><<<grid, dev::kBatchThreads, 0, st>>>(parts, items, nitems, cycles);
+        dev::batch_kernel<float><<<grid, dev::kBatchThreads, 0, st>>>(parts, items, nitems, counter, cycles);
     BCUDA(cudaGetLastError());
     return CSP_OK;
 }
@@ -548,6 +588,7 @@ struct csp_batch {
     std::vector<long long> xoff, yoff, goff;
     Arena arena;
     float *x = nullptr, *y = nullptr, *ybar = nullptr, *xbar = nullptr, *abar = nullptr, *yscratch = nullptr;
+    int* counter = nullptr;   // the persistent kernel's item counter
     std::vector<dev::BatchPart> hparts;      // [fwd(n) | fwd+grad(n) | grad only(n) | adj(n)]
     dev::BatchPart* dparts = nullptr;
     dev::BatchItem* ditems[4] = {nullptr, nullptr, nullptr, nullptr};   // by `what`
@@ -655,6 +696,7 @@ int tune_classes(const std::vector<HCsr>& A, const std::vector<HCsr>& AT, const 
             }
         const size_t o_items = ar.stage(items);
         const size_t o_cyc = ar.take(hp.size() * 8);
+        const size_t o_ctr = ar.take(sizeof(int));
         if ((rc = ar.commit())) break;
         std::vector<dev::BatchPart> d;
         for (int q = 0; q < (int)hp.size(); q++) {
@@ -672,13 +714,14 @@ int tune_classes(const std::vector<HCsr>& A, const std::vector<HCsr>& AT, const 
         auto* parts = reinterpret_cast<const dev::BatchPart*>(ar.base + o_parts);
         auto* ditems = reinterpret_cast<const dev::BatchItem*>(ar.base + o_items);
         auto* cyc = reinterpret_cast<unsigned long long*>(ar.base + o_cyc);
-        rc = launch_batch(bf16, parts, ditems, (int)items.size(), nullptr, grid, st);
+        auto* ctr = reinterpret_cast<int*>(ar.base + o_ctr);
+        rc = launch_batch(bf16, parts, ditems, (int)items.size(), ctr, nullptr, grid, st);
         if (!rc) {
             e = cudaMemsetAsync(cyc, 0, hp.size() * 8, st);
             if (e != cudaSuccess) rc = cuda_error(e, "batch tuning");
         }
         const int reps = 3;
-        for (int k = 0; k < reps && !rc; k++) rc = launch_batch(bf16, parts, ditems, (int)items.size(), cyc, grid, st);
+        for (int k = 0; k < reps && !rc; k++) rc = launch_batch(bf16, parts, ditems, (int)items.size(), ctr, cyc, grid, st);
         std::vector<unsigned long long> hc(hp.size());
         if (!rc) {
             e = cudaMemcpyAsync(hc.data(), cyc, hp.size() * 8, cudaMemcpyDeviceToHost, st);
@@ -851,6 +894,7 @@ int csp_batch_create(const coo_matrix_if* const* mats, int n, const csp_batch_op
         o_ys = ar.take(ny * 4 + 16);
     }
     const size_t o_parts = ar.take((size_t)4 * n * sizeof(dev::BatchPart));
+    const size_t o_ctr = ar.take(sizeof(int));
     const int whats[3] = {CSP_BATCH_FWD, CSP_BATCH_ADJ, CSP_BATCH_FWD | CSP_BATCH_ADJ};
     size_t o_items[4] = {0, 0, 0, 0};
     for (int w : whats) {
@@ -863,6 +907,7 @@ int csp_batch_create(const coo_matrix_if* const* mats, int n, const csp_batch_op
     char* base = ar.base;
     b->x = reinterpret_cast<float*>(base + o_x);
     b->y = reinterpret_cast<float*>(base + o_y);
+    b->counter = reinterpret_cast<int*>(base + o_ctr);
     if (b->adjoint) {
         b->ybar = reinterpret_cast<float*>(base + o_yb);
         b->xbar = reinterpret_cast<float*>(base + o_xb);
@@ -967,7 +1012,7 @@ int csp_batch_run(csp_batch* b, int what, int ntimes)
     cudaStream_t st = b->stream;
     if (!b->use_graph) {
         for (int k = 0; k < ntimes; k++) {
-            int rc = launch_batch(b->bf16, b->dparts, b->ditems[what], b->nitems[what], nullptr, b->grid[what], st);
+            int rc = launch_batch(b->bf16, b->dparts, b->ditems[what], b->nitems[what], b->counter, nullptr, b->grid[what], st);
             if (rc) return rc;
         }
         return CSP_OK;
@@ -976,7 +1021,7 @@ int csp_batch_run(csp_batch* b, int what, int ntimes)
         if (b->graph[what]) { cudaGraphExecDestroy(b->graph[what]); b->graph[what] = nullptr; }
         cudaGraph_t g;
         BCUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        int rc = launch_batch(b->bf16, b->dparts, b->ditems[what], b->nitems[what], nullptr, b->grid[what], st);
+        int rc = launch_batch(b->bf16, b->dparts, b->ditems[what], b->nitems[what], b->counter, nullptr, b->grid[what], st);
         cudaError_t e = cudaStreamEndCapture(st, &g);
         if (rc) { if (e == cudaSuccess) cudaGraphDestroy(g); return rc; }
         if (e != cudaSuccess) return cuda_error(e, "cudaStreamEndCapture");

@@ -341,20 +341,22 @@ int Engine::add_xpanel(const int* rows, const int* cols, const float* vals, int 
     for (int q = 0; q < P; q++)
         for (long long j = cnt[q]; j < cnt[q + 1]; j++)
             if (starts_run(j, cnt[q])) nruns[rows[order[(size_t)j]]]++;
-    // listed rows (rows with entries) and their slot ranges
+    // rows of one run add it to y from the main kernel (one writer, no slot); the
+    // others are listed with their slot ranges for the merge
     std::vector<int> run_ptr, run_rows;
     std::vector<long long> first((size_t)height, -1);
     run_ptr.push_back(0);
     long long total = 0;
     for (int r = 0; r < height; r++) {
-        if (!nruns[r]) continue;
+        if (nruns[r] < 2) continue;
         first[r] = total;
         total += nruns[r];
         run_rows.push_back(r);
         run_ptr.push_back((int)total);
     }
     if (total >= INT32_MAX) return set_error(CSP_EUNSUP, "x-panel part: too many runs");
-    // per-entry slots, panel-local columns and values in tile order
+    // per-entry slots (or -(row + 1) for a one-run row), panel-local columns and values
+    // in tile order
     std::vector<int> slot(slots_len, 0);
     std::vector<unsigned short> lcol(slots_len, 0);
     std::vector<float> val(slots_len, 0.0f);
@@ -364,7 +366,7 @@ int Engine::add_xpanel(const int* rows, const int* cols, const float* vals, int 
         int cur = 0;
         for (long long j = b; j < e; j++) {
             const int i = order[(size_t)j];
-            if (starts_run(j, b)) cur = (int)(first[rows[i]]++);
+            if (starts_run(j, b)) cur = nruns[rows[i]] == 1 ? -(rows[i] + 1) : (int)(first[rows[i]]++);
             slot[o + (size_t)(j - b)] = cur;
             lcol[o + (size_t)(j - b)] = (unsigned short)(cols[i] - q * p.panel_w);
             val[o + (size_t)(j - b)] = vals[i];
@@ -387,7 +389,7 @@ int Engine::add_xpanel(const int* rows, const int* cols, const float* vals, int 
         (rc = alloc(reinterpret_cast<void**>(&p.lcol), slots_len * sizeof(unsigned short))) ||
         (rc = upload_int(&p.tile0, tile0.data(), tile0.size(), tile0.size())) ||
         (rc = upload_int(&p.run_ptr, run_ptr.data(), run_ptr.size(), run_ptr.size())) ||
-        (rc = alloc(reinterpret_cast<void**>(&p.partial), (size_t)total * sizeof(float))))
+        (rc = alloc(reinterpret_cast<void**>(&p.partial), std::max<size_t>((size_t)total, 1) * sizeof(float))))
         return rc;
     CSP_CUDA(cudaMemcpy(p.lcol, lcol.data(), slots_len * sizeof(unsigned short), cudaMemcpyHostToDevice));
     if (!all_rows && (rc = upload_int(&p.run_rows, run_rows.data(), run_rows.size(), run_rows.size()))) return rc;
@@ -858,9 +860,10 @@ static void launch_part(const Part& p, const float* x, float* y, int n, cudaStre
     }
     case PART_XPANEL: {
         dev::xpanel_kernel<V><<<p.ncta, kXpThreads, p.smem, st>>>(
-            p.tile0, p.ntiles, p.npanels, p.i0, p.lcol, v, x, n, p.panel_w, p.partial);
+            p.tile0, p.ntiles, p.npanels, p.i0, p.lcol, v, x, n, p.panel_w, p.partial, y);
+        // at least one CTA even when every row has one run: the launch count stays fixed
         const long long mthreads = (long long)grid_for(p.nrun_rows, 256) * 256 + (long long)p.nlong * kXpMergeLanes;
-        xpanel_merge_kernel<<<grid_for(mthreads, 256), 256, 0, st>>>(p.run_ptr, p.run_rows, p.nrun_rows, p.long_list,
+        xpanel_merge_kernel<<<grid_for(std::max(mthreads, 1LL), 256), 256, 0, st>>>(p.run_ptr, p.run_rows, p.nrun_rows, p.long_list,
                                                                      p.nlong, p.partial, y);
         break;
     }

@@ -28,6 +28,12 @@ int write_sbell(const BlockRows& b, unsigned bw, unsigned bh, unsigned sh, const
 bool quicksort_coo(int* row, int* col, float* val, int n);
 bool coo_is_sorted(const coo_matrix_if* m);
 int autotune_partition(coo_matrix_if* coo, cocktail_iif* out, const csp_analyze_opts* opts);
+
+// The analyzer's counting passes on the current device (analyze_device.cu).
+struct BlockCounts { int partial_blocks, partial_nnz, full_blocks, full_nnz; };
+int device_count_dia(const int* row, const int* col, int nnz, int threshold, std::vector<int>& count);
+int device_count_blocks(const int* rp, const int* col, int h, int nnz, const int* bh, const int* bw, const int* threshold,
+                        int nshapes, std::vector<std::vector<BlockCounts>>& out);
 int ensure_sorted(coo_matrix_if* m);
 
 }  // namespace csp

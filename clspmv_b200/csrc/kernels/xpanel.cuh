@@ -8,14 +8,16 @@
 //     memory); the part's nonzeros are regrouped by panel, keeping row order inside
 //     each panel, and every panel is padded to whole tiles of kXpTile entries;
 //   * inside one tile, a "run" is a maximal group of consecutive entries of one row.
-//     Every run owns one slot of a partial-sum array; slots are numbered row by row
-//     and, inside a row, in panel order.  Pad entries extend the panel's last run
+//     A row with one run in all adds that run to y[row] directly (its entries carry
+//     the code -(row + 1)): it is the row's only writer in the launch.  Every run of
+//     the other rows owns one slot of a partial-sum array; slots are numbered row by
+//     row and, inside a row, in panel order.  Pad entries extend the panel's last run
 //     (value 0, column 0);
-//   * per entry: the slot id of its run (int32), the column inside its panel
-//     (uint16) and the value (FP32 or BF16);
+//   * per entry: the slot id of its run, or the direct-row code (int32), the column
+//     inside its panel (uint16) and the value (FP32 or BF16);
 //   * run_ptr[i]..run_ptr[i+1] are the slots of the i-th listed row: every row with
-//     entries, in order (run_rows[i] is that row, or i itself when every row has
-//     entries).  long_list holds the listed rows with more than kXpShortRuns slots.
+//     two or more runs, in order (run_rows[i] is that row, or i itself when every row
+//     is listed).  long_list holds the listed rows with more than kXpShortRuns slots.
 //
 // xpanel_kernel: each CTA takes an equal share of the tiles (tiles are ordered panel
 // by panel); for each panel its share touches it copies that panel of x into shared
@@ -93,12 +95,23 @@ template <> __device__ __forceinline__ float4 xp_vals<__nv_bfloat16>(const XpSta
                        __uint_as_float(u.y & 0xffff0000u));
 }
 
+// The sum of a closed run: to its slot, or added to y for a one-run row (code
+// -(row + 1)).  The add is a reduction store (no value returned, so the warp does not
+// wait on y); the row has no other writer in the launch, so y_row + v is exact and
+// deterministic.
+__device__ __forceinline__ void xp_close(int key, float v, float* __restrict__ partial, float* __restrict__ y)
+{
+    if (key >= 0) partial[key] = v;
+    else atomicAdd(y + (-key - 1), v);
+}
+
 template <class V>
 __global__ void __launch_bounds__(kXpThreads, 1) xpanel_kernel(const int* __restrict__ tile0, int ntiles, int npanels,
                                                                const int* __restrict__ slot,
                                                                const unsigned short* __restrict__ lcol,
                                                                const V* __restrict__ val, const float* __restrict__ x,
-                                                               int n, int panel_w, float* __restrict__ partial)
+                                                               int n, int panel_w, float* __restrict__ partial,
+                                                               float* __restrict__ y)
 {
     extern __shared__ __align__(16) unsigned char xp_smem[];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -166,13 +179,13 @@ __global__ void __launch_bounds__(kXpThreads, 1) xpanel_kernel(const int* __rest
                 const int prev_key = __shfl_up_sync(0xffffffffu, s.w, 1);
                 float run = (lane > 0 && prev_key == s.x) ? prev_scan : 0.0f;
                 run += p0;
-                if (s.y != s.x) { partial[s.x] = run; run = 0.0f; }
+                if (s.y != s.x) { xp_close(s.x, run, partial, y); run = 0.0f; }
                 run += p1;
-                if (s.z != s.y) { partial[s.y] = run; run = 0.0f; }
+                if (s.z != s.y) { xp_close(s.y, run, partial, y); run = 0.0f; }
                 run += p2;
-                if (s.w != s.z) { partial[s.z] = run; run = 0.0f; }
+                if (s.w != s.z) { xp_close(s.z, run, partial, y); run = 0.0f; }
                 run += p3;
-                if (lane == 31 || next_first != s.w) partial[s.w] = run;
+                if (lane == 31 || next_first != s.w) xp_close(s.w, run, partial, y);
             }
             cp_async_wait<0>();   // only empty groups remain; keeps the accounting clean per panel
             __syncthreads();      // every warp is done with this panel before the next overwrites it

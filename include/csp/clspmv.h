@@ -288,8 +288,14 @@ typedef struct csp_analyze_opts {
     const char* bench_path;  /* REFERENCE: directory holding benchmark/ *.ben; NULL = $CLSPMVPATH */
     int verbose;             /* AUTOTUNE: 1 = print each candidate's measured time        */
     const char* cache_path;  /* AUTOTUNE: file caching decisions per sparsity signature  */
-    int flags;               /* AUTOTUNE: engine flags the partition is tuned for (CSP_FLAG_BF16) */
+    int flags;               /* AUTOTUNE: engine flags the partition is tuned for (CSP_FLAG_BF16);
+                                REFERENCE: CSP_ANALYZE_ON_DEVICE                              */
 } csp_analyze_opts;
+/* REFERENCE mode: the analyzer's integer counting passes -- nonzeros per diagonal
+ * (analyze.cpp:804 count_dia_nnz) and blocks per block row for the eight b4 shapes
+ * (:1582 count_blocks) -- run on the current CUDA device; the partition is the same,
+ * byte for byte.  CSP_ENODEV without a device.  No counterpart in the reference. */
+#define CSP_ANALYZE_ON_DEVICE 0x100
 
 /* Partition `coo` into the per-format sub-matrices of `mat`.  `coo` may be
  * sorted in place (as the reference does).  opts may be NULL (REFERENCE mode,
