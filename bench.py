@@ -527,8 +527,10 @@ def run_batch(dev, args, world, rank, with_cpu: bool):
     load()
     BOTH = CSP_BATCH_FWD | CSP_BATCH_ADJ
     step = lambda: bt.run(BOTH)  # noqa: E731
-    partition = "batch: " + ", ".join(f"{n} x{bt.formats.count(i)}" for i, n in enumerate(BFMT_NAMES)
-                                      if bt.formats.count(i))
+    partition = ("batch: " + ", ".join(f"{n} x{bt.formats.count(i)}" for i, n in enumerate(BFMT_NAMES)
+                                       if bt.formats.count(i))
+                 + "; transposes: " + ", ".join(f"{n} x{bt.formats_adjoint.count(i)}" for i, n in enumerate(BFMT_NAMES)
+                                                if bt.formats_adjoint.count(i)))
 
     # --- timed region: K steps, CUDA events on the launching stream ---
     if world > 1:

@@ -51,6 +51,11 @@ class Batch:
         f = (C.c_int * self.n)()
         check(lib().csp_batch_formats(self.h, f), "batch_formats")
         self.formats = list(f)
+        self.formats_adjoint = None
+        if flags & capi.CSP_FLAG_ADJOINT:
+            ft = (C.c_int * self.n)()
+            check(lib().csp_batch_formats_adjoint(self.h, ft), "batch_formats_adjoint")
+            self.formats_adjoint = list(ft)
 
     def _len(self, which: int) -> int:
         if which in (CSP_BV_X, CSP_BV_XBAR):

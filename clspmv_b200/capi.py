@@ -239,6 +239,7 @@ def _declare(lib):
         "csp_batch_create": (C.c_int, [P(P(coo_matrix)), C.c_int, P(csp_batch_opts), P(C.c_void_p)]),
         "csp_batch_free": (C.c_int, [C.c_void_p]),
         "csp_batch_layout": (C.c_int, [C.c_void_p, P(C.c_longlong), P(C.c_longlong), P(C.c_longlong)]),
+        "csp_batch_formats_adjoint": (C.c_int, [C.c_void_p, P(C.c_int)]),
         "csp_batch_formats": (C.c_int, [C.c_void_p, IP]),
         "csp_batch_device_ptrs": (C.c_int, [C.c_void_p, P(C.c_void_p), P(C.c_void_p), P(C.c_void_p), P(C.c_void_p),
                                             P(C.c_void_p)]),

@@ -150,11 +150,13 @@ void features(const HCsr& c, int flags, csp_batch_features& f)
         f.bcsr_blocks[b - 2] = blocks;
     }
     // candidates: CSR always; the padded formats while they store at most 1.5x the entries
-    const double lim = 1.5 * nnz + 64;
+    // (sliced ELL: 2x, since its per-row lane needs no reduction and short, even rows --
+    // the transposes of long-row matrices -- often come just above 1.5x)
+    const double lim = 1.5 * nnz + 64, sell_lim = 2.0 * nnz + 64;
     unsigned feas = 1u << CSP_BFMT_CSR;
     if (nnz > 0) {
-        if (f.sell_slots[0] <= lim && f.sell_slots[0] < INT_MAX) feas |= 1u << CSP_BFMT_SELL32;
-        if (f.sell_slots[1] <= lim && f.sell_slots[1] < INT_MAX) feas |= 1u << CSP_BFMT_SELL128;
+        if (f.sell_slots[0] <= sell_lim && f.sell_slots[0] < INT_MAX) feas |= 1u << CSP_BFMT_SELL32;
+        if (f.sell_slots[1] <= sell_lim && f.sell_slots[1] < INT_MAX) feas |= 1u << CSP_BFMT_SELL128;
         if (dia_ok && (double)offs.size() * m <= lim && f.dia_slots < INT_MAX) feas |= 1u << CSP_BFMT_DIA;
         for (int b = 2; b <= 4; b++)
             if ((double)f.bcsr_blocks[b - 2] * b * b <= lim && f.bcsr_blocks[b - 2] * b * b < INT_MAX)
@@ -584,7 +586,7 @@ struct csp_batch {
     int n = 0;
     int flags = 0;
     bool bf16 = false, adjoint = false, use_graph = false;
-    std::vector<int> fmt;
+    std::vector<int> fmt, fmt_t;   // formats of A and of A^T
     std::vector<long long> xoff, yoff, goff;
     Arena arena;
     float *x = nullptr, *y = nullptr, *ybar = nullptr, *xbar = nullptr, *abar = nullptr, *yscratch = nullptr;
@@ -630,21 +632,24 @@ std::vector<dev::BatchItem> items_for(const csp_batch* b, int what)
     return it;
 }
 
-// Device timing of candidate formats for every signature class that has no cached
-// decision: each round stores up to 4 representative matrices of every class in
-// that round's candidate format and runs the forward+adjoint work list a few times
-// with per-part cycle counters; a class takes the format with the fewest cycles
-// per stored entry.
-int tune_classes(const std::vector<HCsr>& A, const std::vector<HCsr>& AT, const std::vector<csp_batch_features>& F,
-                 int flags, const char* cache_path, std::vector<int>& choice)
+// Device timing of candidate formats for one side of the batch -- the stored matrices
+// A (forward, with the value-gradient store when `grad`) or their transposes A^T
+// (adjoint) -- for every signature class without a cached decision: each round stores
+// up to 4 representative operators of every class in that round's candidate format and
+// runs them in the persistent kernel a few times with per-part cycle counters; a class
+// takes the format with the fewest cycles per stored entry.  `salt` separates the two
+// sides' classes in the decision cache.
+int tune_classes(const std::vector<HCsr>& M, const std::vector<csp_batch_features>& F, bool grad,
+                 unsigned long long salt, int flags, const char* cache_path, std::vector<int>& choice)
 {
     const bool bf16 = (flags & CSP_FLAG_BF16) != 0;
-    const int n = (int)A.size();
+    const int n = (int)M.size();
     std::map<unsigned long long, std::vector<int>> classes;
     for (int i = 0; i < n; i++) {
         int f = -1;
-        if (cache_get(F[i].signature, f)) choice[i] = (F[i].feasible & (1u << f)) ? f : F[i].model_format;
-        else classes[F[i].signature].push_back(i);
+        const unsigned long long sig = F[i].signature ^ salt;
+        if (cache_get(sig, f)) choice[i] = (F[i].feasible & (1u << f)) ? f : F[i].model_format;
+        else classes[sig].push_back(i);
     }
     if (classes.empty()) return CSP_OK;
     struct Cls { unsigned long long sig; std::vector<int> reps; unsigned feas; double cost[CSP_BFMT_COUNT]; };
@@ -668,16 +673,14 @@ int tune_classes(const std::vector<HCsr>& A, const std::vector<HCsr>& AT, const 
         Arena ar;
         std::vector<HPart> hp;
         std::vector<PartOffs> po;
-        std::vector<std::pair<int, int>> owner;   // (class, is adjoint)
+        std::vector<int> owner;   // class of each timed operator
         std::vector<size_t> vx, vy, vg;
         for (int c = 0; c < (int)cls.size(); c++) {
             if (!(cls[c].feas & (1u << fmt))) continue;
             for (int r : cls[c].reps) {
-                for (int adj = 0; adj < 2; adj++) {
-                    hp.emplace_back();
-                    build_part(fmt, adj ? AT[r] : A[r], hp.back());
-                    owner.emplace_back(c, adj);
-                }
+                hp.emplace_back();
+                build_part(fmt, M[r], hp.back());
+                owner.push_back(c);
             }
         }
         if (hp.empty()) continue;
@@ -705,7 +708,7 @@ int tune_classes(const std::vector<HCsr>& A, const std::vector<HCsr>& AT, const 
             bp.y = reinterpret_cast<float*>(ar.base + vy[q]);
             bp.ybar = bp.y;   // any readable vector of the right length
             bp.abar = reinterpret_cast<float*>(ar.base + vg[q]);
-            bp.grad = owner[q].second ? 0 : 1;
+            bp.grad = grad ? 1 : 0;
             d.push_back(bp);
         }
         cudaError_t e = cudaMemcpy(ar.base + o_parts, d.data(), d.size() * sizeof(dev::BatchPart), cudaMemcpyHostToDevice);
@@ -731,7 +734,7 @@ int tune_classes(const std::vector<HCsr>& A, const std::vector<HCsr>& AT, const 
         ar.release();
         if (rc) break;
         std::vector<double> sum(cls.size(), 0.0);
-        for (int q = 0; q < (int)hp.size(); q++) sum[owner[q].first] += (double)hc[q] / reps;
+        for (int q = 0; q < (int)hp.size(); q++) sum[owner[q]] += (double)hc[q] / reps;
         for (int c = 0; c < (int)cls.size(); c++) {
             if (!(cls[c].feas & (1u << fmt))) continue;
             long long nnz = 0;
@@ -819,12 +822,18 @@ int csp_batch_create(const coo_matrix_if* const* mats, int n, const csp_batch_op
         csr_of(mats[i], A[i]);
         features(A[i], o.flags, F[i]);
     }
-    const bool need_t = b->adjoint || (o.format == CSP_BFMT_AUTO && o.tune == CSP_BATCH_TUNE_DEVICE);
+    const bool need_t = b->adjoint;
+    std::vector<csp_batch_features> FT;
     if (need_t) {
         AT.resize((size_t)n);
-        for (int i = 0; i < n; i++) transpose(A[i], AT[i]);
+        FT.resize((size_t)n);
+        for (int i = 0; i < n; i++) {
+            transpose(A[i], AT[i]);
+            features(AT[i], o.flags, FT[i]);
+        }
     }
     b->fmt.assign((size_t)n, CSP_BFMT_CSR);
+    b->fmt_t.assign((size_t)n, CSP_BFMT_CSR);
     b->plain_g.assign((size_t)2 * n, 1);
     for (int i = 0; i < n; i++) {
         const double nz = F[i].nnz;
@@ -835,17 +844,24 @@ int csp_batch_create(const coo_matrix_if* const* mats, int n, const csp_batch_op
             b->plain_g[2 * i + t] = g;
         }
     }
+    // A and A^T choose their formats independently (A^T of a matrix with long rows has
+    // short, even ones); a forced format applies to both
     if (o.format != CSP_BFMT_AUTO) {
         for (int i = 0; i < n; i++) {
             if (!(F[i].feasible & (1u << o.format)))
                 return set_error(CSP_EFORMAT, "batch matrix %d: format %d not feasible", i, o.format);
-            b->fmt[i] = o.format;
+            b->fmt[i] = b->fmt_t[i] = o.format;
         }
     } else if (o.tune == CSP_BATCH_TUNE_MODEL) {
-        for (int i = 0; i < n; i++) b->fmt[i] = F[i].model_format;
+        for (int i = 0; i < n; i++) {
+            b->fmt[i] = F[i].model_format;
+            if (need_t) b->fmt_t[i] = FT[i].model_format;
+        }
     } else {
         cache_read(o.cache_path);
-        if ((rc = tune_classes(A, AT, F, o.flags, o.cache_path, b->fmt))) return rc;
+        if ((rc = tune_classes(A, F, b->adjoint, 0ULL, o.flags, o.cache_path, b->fmt))) return rc;
+        if (need_t && (rc = tune_classes(AT, FT, false, 0x9e3779b97f4a7c15ULL, o.flags, o.cache_path, b->fmt_t)))
+            return rc;
     }
 
     BCUDA(cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking));
@@ -869,7 +885,7 @@ int csp_batch_create(const coo_matrix_if* const* mats, int n, const csp_batch_op
         b->yoff[i + 1] = b->yoff[i] + A[i].m;
         b->goff[i + 1] = b->goff[i] + (b->adjoint ? pad_ll(fw[i].slots, 64) : 0);
         if (b->adjoint) {
-            build_part(b->fmt[i], AT[i], bw[i]);
+            build_part(b->fmt_t[i], AT[i], bw[i]);
             bo[i] = stage_part(ar, bw[i], b->bf16);
             b->ranges_adj[i] = bw[i].ranges;
             bw[i].i0.clear(); bw[i].i0.shrink_to_fit();
@@ -965,6 +981,14 @@ int csp_batch_formats(const csp_batch* b, int* formats)
     return CSP_OK;
 }
 
+int csp_batch_formats_adjoint(const csp_batch* b, int* formats)
+{
+    if (!b || !formats) return set_error(CSP_EINVAL, "null argument");
+    if (!b->adjoint) return set_error(CSP_EUNSUP, "batch built without CSP_FLAG_ADJOINT");
+    memcpy(formats, b->fmt_t.data(), b->fmt_t.size() * sizeof(int));
+    return CSP_OK;
+}
+
 int csp_batch_device_ptrs(const csp_batch* b, float** x, float** y, float** ybar, float** xbar, float** abar)
 {
     if (!b) return set_error(CSP_EINVAL, "null batch");
@@ -1042,6 +1066,9 @@ int csp_batch_run_plain(csp_batch* b, int what, int ntimes, int lanes)
     if ((what & CSP_BATCH_ADJ) && !b->adjoint) return set_error(CSP_EUNSUP, "batch built without CSP_FLAG_ADJOINT");
     for (int f : b->fmt)
         if (f != CSP_BFMT_CSR) return set_error(CSP_EUNSUP, "plain runs need every matrix in CSR");
+    if (b->adjoint)
+        for (int f : b->fmt_t)
+            if (f != CSP_BFMT_CSR) return set_error(CSP_EUNSUP, "plain runs need every transpose in CSR");
     if (lanes != 0 && (lanes < 1 || lanes > 32 || (lanes & (lanes - 1))))
         return set_error(CSP_EINVAL, "lanes must be 0 or a power of two up to 32");
     cudaStream_t st = b->stream;

@@ -75,8 +75,9 @@ constexpr int kBatchItemWords = (int)(sizeof(BatchItem) / 4);
 
 // One warp's shared memory.
 struct WarpSmem {
-    BatchPart part[2];
-    BatchItem item[2];
+    BatchPart part[2];                     // descriptors of the current and the next item
+    BatchItem item[3];                     // words of the current item and the next two
+    int res_next, res_end;                 // items reserved from the counter (lane 0)
     float4 prod[32 * kWarpVecs];           // CSR: the item's products, at entry - 4-aligned start
     int rp[kWarpRows + 1];                 // CSR: the item's row pointers, relative to that start
     float ys[kWarpRows];                   // CSR: the item's y rows
@@ -395,12 +396,23 @@ __device__ __forceinline__ void batch_item(WarpSmem& ws, const BatchPart& P, con
     }
 }
 
+__device__ __forceinline__ void cp_async4(void* dst, const void* src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
+}
+__device__ __forceinline__ void cp_async_commit_wait_all() { asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::); }
+__device__ __forceinline__ void cp_async_commit_group() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::); }
+
 // The warps take items from a shared counter (`next`, zero at launch), kBatchReserve
 // consecutive items per atomic: a warp reserves the item after its next one while it
 // runs the current item, so the items a warp gets follow how long its earlier ones
-// took, and a warp holds at most kBatchReserve + 1 items it has not started.  Which warp runs an item does not change any result.  `cycles`, when
-// non-null, receives per part the SM clock cycles its items held a warp (the
-// autotuner's cost).
+// took, and a warp holds at most kBatchReserve + 1 items it has not started.  The next
+// item's descriptor and the words of the item after it are copied into the warp's
+// shared memory asynchronously (cp.async) while the current item runs, so no register
+// holds them across the item.  Which warp runs an item does not change any result.
+// `cycles`, when non-null, receives per part the SM clock cycles its items held a warp
+// (the autotuner's cost).
 template <class V>
 __global__ void __launch_bounds__(kBatchThreads, 4) batch_kernel(const BatchPart* __restrict__ parts,
                                                                   const BatchItem* __restrict__ items, int nitems,
@@ -412,59 +424,56 @@ __global__ void __launch_bounds__(kBatchThreads, 4) batch_kernel(const BatchPart
     WarpSmem& ws = sm.w[threadIdx.x >> 5];
     const int* __restrict__ iw = reinterpret_cast<const int*>(items);
     const int* __restrict__ pw = reinterpret_cast<const int*>(parts);
-    // items are reserved kBatchReserve at a time (one counter atomic per group)
-    int res_next = 0, res_end = 0;
     auto reserve = [&]() {
-        if (res_next == res_end) {
-            int v = 0;
-            if (lane == 0) v = atomicAdd(next, kBatchReserve);
-            res_next = __shfl_sync(0xffffffffu, v, 0);
-            res_end = res_next + kBatchReserve;
+        int v = 0;
+        if (lane == 0) {
+            if (ws.res_next == ws.res_end) {
+                ws.res_next = atomicAdd(next, kBatchReserve);
+                ws.res_end = ws.res_next + kBatchReserve;
+            }
+            v = ws.res_next++;
         }
-        return res_next++;
+        return __shfl_sync(0xffffffffu, v, 0);
     };
+    if (lane == 0) ws.res_next = ws.res_end = 0;
+    __syncwarp();
     int it = reserve();
     if (it >= nitems) return;   // the whole warp leaves together
-    // prologue: item `it` and its descriptor into buffer 0
+    // prologue: item `it` and its descriptor into slots 0, the next item's words in flight
     if (lane < kBatchItemWords) reinterpret_cast<int*>(&ws.item[0])[lane] = __ldg(iw + (size_t)it * kBatchItemWords + lane);
     if (lane < kBatchPartWords) {
         const int px = __ldg(iw + (size_t)it * kBatchItemWords);
         reinterpret_cast<int*>(&ws.part[0])[lane] = __ldg(pw + (size_t)px * kBatchPartWords + lane);
     }
-    // registers: the next item and its words
     int n1 = reserve();
-    int nw = 0, npx = 0;
-    if (n1 < nitems) {
-        if (lane < kBatchItemWords) nw = __ldg(iw + (size_t)n1 * kBatchItemWords + lane);
-        if (lane < kBatchPartWords) npx = __ldg(iw + (size_t)n1 * kBatchItemWords);
-    }
+    if (n1 < nitems && lane < kBatchItemWords)
+        cp_async4(reinterpret_cast<int*>(&ws.item[1]) + lane, iw + (size_t)n1 * kBatchItemWords + lane);
+    cp_async_commit_wait_all();
     __syncwarp();
-    int b = 0;
+    int ib = 0, pb = 0;
     while (true) {
-        // one ahead: the next item's descriptor; two ahead: reserve an item, load its words
+        // the next item's words have landed: its descriptor, and the words of the one after
+        const int ib1 = ib == 2 ? 0 : ib + 1, ib2 = ib1 == 2 ? 0 : ib1 + 1;
         const int n2 = n1 < nitems ? reserve() : nitems;
-        int pword = 0, nw2 = 0, npx2 = 0;
-        if (n1 < nitems && lane < kBatchPartWords) pword = __ldg(pw + (size_t)npx * kBatchPartWords + lane);
-        if (n2 < nitems) {
-            if (lane < kBatchItemWords) nw2 = __ldg(iw + (size_t)n2 * kBatchItemWords + lane);
-            if (lane < kBatchPartWords) npx2 = __ldg(iw + (size_t)n2 * kBatchItemWords);
-        }
+        if (n1 < nitems && lane < kBatchPartWords)
+            cp_async4(reinterpret_cast<int*>(&ws.part[pb ^ 1]) + lane, pw + (size_t)ws.item[ib1].part * kBatchPartWords + lane);
+        if (n2 < nitems && lane < kBatchItemWords)
+            cp_async4(reinterpret_cast<int*>(&ws.item[ib2]) + lane, iw + (size_t)n2 * kBatchItemWords + lane);
+        cp_async_commit_group();
         long long t0 = 0;
         if (cycles && lane == 0) t0 = clock64();
-        const BatchPart& P = ws.part[b];
-        if (P.grad) batch_item<V, true>(ws, P, ws.item[b], lane);
-        else batch_item<V, false>(ws, P, ws.item[b], lane);
-        if (cycles && lane == 0) atomicAdd(cycles + ws.item[b].part, (unsigned long long)(clock64() - t0));
+        const BatchPart& P = ws.part[pb];
+        if (P.grad) batch_item<V, true>(ws, P, ws.item[ib], lane);
+        else batch_item<V, false>(ws, P, ws.item[ib], lane);
+        if (cycles && lane == 0) atomicAdd(cycles + ws.item[ib].part, (unsigned long long)(clock64() - t0));
         if (n1 >= nitems) break;
+        cp_async_wait_all();
         __syncwarp();
-        if (lane < kBatchItemWords) reinterpret_cast<int*>(&ws.item[b ^ 1])[lane] = nw;
-        if (lane < kBatchPartWords) reinterpret_cast<int*>(&ws.part[b ^ 1])[lane] = pword;
-        __syncwarp();
-        nw = nw2;
-        npx = npx2;
         n1 = n2;
-        b ^= 1;
+        ib = ib1;
+        pb ^= 1;
     }
+    cp_async_wait_all();   // no copy is left in flight when the warp leaves
 }
 
 // Value gradient of a plain CSR matrix, one warp per row: abar[j] = ybar[row] * x[col[j]].

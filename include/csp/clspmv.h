@@ -524,6 +524,9 @@ int csp_batch_free(csp_batch* b);
 /* n + 1 prefix offsets each (floats); any pointer may be NULL. */
 int csp_batch_layout(const csp_batch* b, long long* x_off, long long* y_off, long long* abar_off);
 int csp_batch_formats(const csp_batch* b, int* formats);
+/* Formats of the stored transposes A_i^T (CSP_FLAG_ADJOINT batches): chosen on their own,
+ * since the transpose of a matrix with long rows has short, even rows. */
+int csp_batch_formats_adjoint(const csp_batch* b, int* formats);
 int csp_batch_device_ptrs(const csp_batch* b, float** x, float** y, float** ybar, float** xbar, float** abar);
 /* Whole-vector copies on the batch stream: host `src` -> device, or device -> host
  * `dst` (then synchronised).  Exactly one of src, dst is non-NULL. */

@@ -38,12 +38,12 @@ def _expected(case, bf16=False):
         key = np.unique((r.astype(np.int64) // b) * (w + b) + (c - c % b))
         blocks.append(int(key.size))
     f["bcsr_blocks"] = blocks
-    lim = 1.5 * nnz + 64
+    lim, sell_lim = 1.5 * nnz + 64, 2.0 * nnz + 64
     feas = 1 << CSP_BFMT_CSR
     if nnz:
-        if sell[0] <= lim:
+        if sell[0] <= sell_lim:
             feas |= 1 << CSP_BFMT_SELL32
-        if sell[1] <= lim:
+        if sell[1] <= sell_lim:
             feas |= 1 << CSP_BFMT_SELL128
         if ndiag >= 0 and ndiag * h <= lim:
             feas |= 1 << CSP_BFMT_DIA

@@ -52,15 +52,18 @@ def _merged(case):
     return h, w, (uk // max(w, 1)).astype(np.int32), (uk % max(w, 1)).astype(np.int32), acc
 
 
-def _oracle_all(case, x, y0, ybar, xbar0, vals=None):
-    h, w, r, c, v = case
-    if vals is not None:
-        v = vals
-    order = np.lexsort((c, r))
-    r, c, v = r[order], c[order], v[order]
-    rp = csr_from_coo(h, r)
-    fy, by = _oracle.fp64_spmv(h, w, rp, c, v, x, None)
-    fx, bx = _oracle.fp64_spmv(h, w, rp, c, v, ybar, None, transpose=True)
+def _oracle_all(case, x, y0, ybar, xbar0, vals=None, case_t=None, vals_t=None):
+    """FP64 references of y0 + A x and xbar0 + A^T ybar; the transposed product uses
+    case_t / vals_t (the matrix as the A^T part stores it) where given."""
+    def prod(cs, vv, vec, transpose):
+        h, w, r, c, v = cs
+        if vv is not None:
+            v = vv
+        order = np.lexsort((c, r))
+        r, c, v = r[order], c[order], v[order]
+        return _oracle.fp64_spmv(h, w, csr_from_coo(h, r), c, v, vec, None, transpose=transpose)
+    fy, by = prod(case, vals, x, False)
+    fx, bx = prod(case_t if case_t is not None else case, vals_t if case_t is not None else vals, ybar, True)
     return (y0 + fy, _oracle.y0_term(y0) + by), (xbar0 + fx, _oracle.y0_term(xbar0) + bx)
 
 
@@ -106,12 +109,17 @@ class Run:
         worst = 0.0
         for i, (name, case) in enumerate(zip(self.names, self.cases)):
             xs, ys = self.sl(self.b.x_off, i), self.sl(self.b.y_off, i)
-            vals = None
+            vals = vals_t = case_t = None
             if bf16:
-                if self.b.formats[i] not in (CSP_BFMT_CSR, CSP_BFMT_SELL32, CSP_BFMT_SELL128):
+                # DIA and BCSR parts store duplicates summed, then rounded to BF16
+                flat = (CSP_BFMT_CSR, CSP_BFMT_SELL32, CSP_BFMT_SELL128)
+                fa = self.b.formats[i]
+                ft = self.b.formats_adjoint[i] if self.b.formats_adjoint else fa
+                case_t = _merged(case) if ft not in flat else case
+                if fa not in flat:
                     case = _merged(case)
-                vals = _bf16(case[4])
-            ry, rx = _oracle_all(case, self.x[xs], self.y0[ys], self.ybar[ys], self.xbar0[xs], vals)
+                vals, vals_t = _bf16(case[4]), _bf16(case_t[4])
+            ry, rx = _oracle_all(case, self.x[xs], self.y0[ys], self.ybar[ys], self.xbar0[xs], vals, case_t, vals_t)
             if what & CSP_BATCH_FWD:
                 e = _err(y[ys], ry)
                 assert e <= tol, f"{name} ({BFMT_NAMES[self.b.formats[i]]}): forward error {e:.3e}"
@@ -169,6 +177,7 @@ def test_model_choice_and_directions():
     run = Run(names)
     model = [features(COO(*CASES[n]))["model_format"] for n in names]
     assert run.b.formats == model
+    assert len(run.b.formats_adjoint) == len(names)
     run.b.run(CSP_BATCH_FWD)
     run.check(CSP_BATCH_FWD)
     xbar = run.b.copy_out(CSP_BV_XBAR)
