@@ -24,6 +24,7 @@ CSP_FLAG_TENSOR_CORES = 0x20
 CSP_METH_XPANEL = 16
 CSP_METH_GENERIC_BCSR = 32
 CSP_ANALYZE_ON_DEVICE = 0x100
+CSP_MMF_SORT_ON_DEVICE = 0x1
 CSP_ANALYZE_REFERENCE, CSP_ANALYZE_AUTOTUNE = 0, 1
 CSP_NOALLOC_MAX_NNZ = 33554432
 CSP_BFMT_AUTO = -1
@@ -228,6 +229,8 @@ def _declare(lib):
         "csp_evaluate": (C.c_int, [P(cocktail), FP, FP, FP, C.c_int, P(csp_report)]),
         "csp_spmv_all": (C.c_int, [P(coo_matrix), C.c_int, C.c_int, P(csp_report)]),
         "csp_read_mmf": (C.c_int, [C.c_char_p, P(coo_matrix)]),
+        "csp_read_mmf_ex": (C.c_int, [C.c_char_p, P(coo_matrix), C.c_int]),
+        "csp_sort_coo_device": (C.c_int, [P(coo_matrix)]),
         "csp_autotune_choice": (C.c_char_p, []),
         "csp_bandwidth_test": (C.c_int, [C.c_size_t, C.c_int, P(csp_bandwidth_report)]),
         "csp_spmv_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

@@ -279,7 +279,9 @@ int csp_spmv_sbell(coo_matrix_if* c, int n, csp_report* r) { return csp_spmv_all
 // comment lines, "rows cols nnz", then 1-based entries.  Pattern matrices get 1.0;
 // symmetric ones are mirrored (diagonal once) and sorted; general ones sorted if needed.
 // Unlike the reference, an "integer" field's values are read rather than misparsed.
-int csp_read_mmf(const char* filename, coo_matrix_if* mat)
+int csp_read_mmf(const char* filename, coo_matrix_if* mat) { return csp_read_mmf_ex(filename, mat, 0); }
+
+int csp_read_mmf_ex(const char* filename, coo_matrix_if* mat, int flags)
 {
     if (!filename || !mat) return set_error(CSP_EINVAL, "null argument");
     FILE* f = fopen(filename, "r");
@@ -328,6 +330,7 @@ int csp_read_mmf(const char* filename, coo_matrix_if* mat)
         mat->coo_row_id[k] = r[i]; mat->coo_col_id[k] = c[i]; mat->coo_data[k] = v[i]; k++;
         if (sym && r[i] != c[i]) { mat->coo_row_id[k] = c[i]; mat->coo_col_id[k] = r[i]; mat->coo_data[k] = v[i]; k++; }
     }
+    if (flags & CSP_MMF_SORT_ON_DEVICE) return coo_is_sorted(mat) ? CSP_OK : csp_sort_coo_device(mat);
     if (sym) return csp_sort_coo(mat);
     return ensure_sorted(mat);
 }

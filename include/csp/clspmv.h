@@ -597,6 +597,17 @@ int csp_bandwidth_test(size_t bytes, int gather_range, csp_bandwidth_report* rep
 /* symmetric mirrored, sorted.                                               */
 /* ------------------------------------------------------------------------ */
 int csp_read_mmf(const char* filename, coo_matrix_if* mat);
+/* csp_read_mmf with options.  CSP_MMF_SORT_ON_DEVICE: the entries are sorted by
+ * (row, col) on the current CUDA device (csp_sort_coo_device) instead of the host.
+ * No counterpart in the reference. */
+#define CSP_MMF_SORT_ON_DEVICE 0x1
+int csp_read_mmf_ex(const char* filename, coo_matrix_if* mat, int flags);
+/* A host COO sorted in place by (row, col) on the current CUDA device: a stable radix
+ * sort, so entries with equal (row, col) keep their input order (the reference's
+ * quicksort, matrix_storage.h:745, may order such duplicates differently; without
+ * duplicates the two agree byte for byte).  CSP_ENODEV without a device.  No
+ * counterpart in the reference. */
+int csp_sort_coo_device(coo_matrix_if* mat);
 
 #if defined(__GNUC__)
 #pragma GCC visibility pop
