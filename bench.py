@@ -382,19 +382,64 @@ def cpu_baseline(mats, x, y0, nbytes, budget_s, adjoint=False, ybar=None, gpu_y=
 # device timing
 # ---------------------------------------------------------------------------
 class ClockSampler:
-    """nvidia-smi SM clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: NVML read every
+    5 ms from a thread (the timed regions are tens of milliseconds), else nvidia-smi
+    every 100 ms.  Read-only queries; nothing of the GPU's settings changes."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
         self.lines = []
         self.thread = None
+        self.nvml = None
+        self.samples = []   # (sm MHz, reason bits)
+        self.smax = None
+        self.running = False
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.device)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
+
+    def _nvml_sample(self):
+        nv, h = self.nvml
+        try:
+            bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        except Exception:
+            bits = nv.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+        self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)), int(bits)))
+
+    def _nvml_loop(self):
+        while self.running:
+            try:
+                self._nvml_sample()
+            except Exception:
+                return
+            time.sleep(0.005)
 
     def start(self):
+        try:
+            self.nvml = self._nvml_handle()
+            self.smax = float(self.nvml[0].nvmlDeviceGetMaxClockInfo(self.nvml[1], self.nvml[0].NVML_CLOCK_SM))
+            self._nvml_sample()   # the first sample before the timed region starts
+            self.running = True
+            self.thread = threading.Thread(target=self._nvml_loop, daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
@@ -409,6 +454,13 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def stop(self):
+        if self.nvml is not None:
+            self.running = False
+            self.thread.join(timeout=1)
+            sm = [c for c, _ in self.samples]
+            reasons = sorted({nm for _, bits in self.samples for nm, b in self.REASONS if bits & b})
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.smax, "reasons": reasons,
+                    "samples": len(sm), "source": "NVML every 5 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         time.sleep(0.25)
@@ -418,7 +470,7 @@ class ClockSampler:
         except Exception:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        names = [nm for nm, _ in self.REASONS]
         for ln in self.lines:
             p = [t.strip() for t in ln.split(",")]
             if len(p) < 9:
@@ -432,7 +484,7 @@ class ClockSampler:
                 if val.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvidia-smi every 100 ms"}
 
 
 class Device:

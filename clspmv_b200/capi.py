@@ -231,6 +231,9 @@ def _declare(lib):
         "csp_read_mmf": (C.c_int, [C.c_char_p, P(coo_matrix)]),
         "csp_read_mmf_ex": (C.c_int, [C.c_char_p, P(coo_matrix), C.c_int]),
         "csp_sort_coo_device": (C.c_int, [P(coo_matrix)]),
+        "csp_coo2dia_device": (C.c_int, [P(coo_matrix), P(dia_matrix), C.c_int]),
+        "csp_coo2bdia_device": (C.c_int, [P(coo_matrix), P(bdia_matrix), C.c_int]),
+        "csp_coo2bcsr_device": (C.c_int, [P(coo_matrix), P(bcsr_matrix), C.c_uint, C.c_uint, C.c_int]),
         "csp_autotune_choice": (C.c_char_p, []),
         "csp_bandwidth_test": (C.c_int, [C.c_size_t, C.c_int, P(csp_bandwidth_report)]),
         "csp_spmv_adjoint": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),

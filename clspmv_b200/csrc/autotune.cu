@@ -192,7 +192,13 @@ int build(const Coo& a, const std::string& name, cocktail_iif* c)
     if (sscanf(name.c_str(), "gbcsr%dx%d", &x, &y) == 2) {
         c->ifusebcsr = true;
         c->bcsr_meth_num = CSP_METH_GENERIC_BCSR;
-        return csp_coo2bcsr(m, reinterpret_cast<bcsr_matrix_if*>(&c->bcsr), (unsigned)y, (unsigned)x, 32);
+        // built on the device unless duplicate entries make the host build's choice
+        // among them the byte-exact one
+        auto* gb = reinterpret_cast<bcsr_matrix_if*>(&c->bcsr);
+        int rc = ensure_sorted(m);
+        if (rc) return rc;
+        return coo_has_duplicates(m) ? csp_coo2bcsr(m, gb, (unsigned)y, (unsigned)x, 32)
+                                     : csp_coo2bcsr_device(m, gb, (unsigned)y, (unsigned)x, 32);
     }
     if (sscanf(name.c_str(), "bcsr%dx%dm%d", &x, &y, &z) == 3) {
         c->ifusebcsr = true;
@@ -210,12 +216,12 @@ int build(const Coo& a, const std::string& name, cocktail_iif* c)
     if (sscanf(name.c_str(), "bdia%d", &x) == 1) {
         c->ifusebdia = true;
         c->bdia_meth_num = x;
-        return csp_coo2bdia(m, &c->bdia, 32);
+        return csp_coo2bdia_device(m, &c->bdia, 32);
     }
     if (sscanf(name.c_str(), "dia%d", &x) == 1) {
         c->ifusedia = true;
         c->dia_meth_num = x;
-        return csp_coo2dia(m, &c->dia, 32);
+        return csp_coo2dia_device(m, &c->dia, 32);
     }
     if (sscanf(name.c_str(), "sell%d", &x) == 1) {
         c->ifusesell = true;

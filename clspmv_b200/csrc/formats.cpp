@@ -122,6 +122,13 @@ bool coo_is_sorted(const coo_matrix_if* m)
     return true;
 }
 
+bool coo_has_duplicates(const coo_matrix_if* m)
+{
+    for (int i = 0; i + 1 < m->matinfo.nnz; i++)
+        if (m->coo_row_id[i] == m->coo_row_id[i + 1] && m->coo_col_id[i] == m->coo_col_id[i + 1]) return true;
+    return false;
+}
+
 int ensure_sorted(coo_matrix_if* m)
 {
     if (coo_is_sorted(m)) return CSP_OK;
@@ -281,6 +288,33 @@ int write_sbell(const BlockRows& b, unsigned bw, unsigned bh, unsigned sh, const
         }
         for (; k < width[sl]; k++) d->sbell_col_id[cstart + lr + (size_t)k * H] = last;
     }
+    return CSP_OK;
+}
+
+// The banding step of coo2bdia (matrix_storage.h:1185): runs of consecutive offsets
+// of a built DIA become bands; the DIA's data moves into the BDIA unchanged (same
+// layout) and the DIA is freed.
+int bdia_from_dia(dia_matrix_iif* dia, bdia_matrix_iif* d)
+{
+    std::vector<int> boff, bcnt;
+    for (int k = 0; k < dia->dia_num; k++) {
+        if (k > 0 && dia->dia_offsets[k] - dia->dia_offsets[k - 1] == 1) bcnt.back()++;
+        else { boff.push_back(dia->dia_offsets[k]); bcnt.push_back(1); }
+    }
+    d->bdia_band_num = (int)boff.size();
+    d->bdia_length = dia->dia_length;
+    d->bdia_length_aligned = dia->dia_length_aligned;
+    d->bdia_offsets = xmalloc<int>(boff.size());
+    d->bdia_bptr = xmalloc<int>(boff.size() + 1);
+    if (!d->bdia_offsets || !d->bdia_bptr) { csp_free_dia_matrix(dia); return set_error(CSP_ENOMEM, "coo2bdia"); }
+    d->bdia_bptr[0] = 0;
+    for (size_t b = 0; b < boff.size(); b++) {
+        d->bdia_offsets[b] = boff[b];
+        d->bdia_bptr[b + 1] = d->bdia_bptr[b] + bcnt[b];
+    }
+    d->bdia_data = dia->dia_data;   // identical data layout
+    dia->dia_data = nullptr;
+    csp_free_dia_matrix(dia);
     return CSP_OK;
 }
 
@@ -550,26 +584,7 @@ int csp_coo2bdia(coo_matrix_if* s, bdia_matrix_iif* d, int alignment)
     int rc = csp_coo2dia(s, &dia, alignment);
     d->matinfo = s ? s->matinfo : d->matinfo;
     if (rc) return rc;
-    std::vector<int> boff, bcnt;
-    for (int k = 0; k < dia.dia_num; k++) {
-        if (k > 0 && dia.dia_offsets[k] - dia.dia_offsets[k - 1] == 1) bcnt.back()++;
-        else { boff.push_back(dia.dia_offsets[k]); bcnt.push_back(1); }
-    }
-    d->bdia_band_num = (int)boff.size();
-    d->bdia_length = dia.dia_length;
-    d->bdia_length_aligned = dia.dia_length_aligned;
-    d->bdia_offsets = xmalloc<int>(boff.size());
-    d->bdia_bptr = xmalloc<int>(boff.size() + 1);
-    if (!d->bdia_offsets || !d->bdia_bptr) { csp_free_dia_matrix(&dia); return set_error(CSP_ENOMEM, "coo2bdia"); }
-    d->bdia_bptr[0] = 0;
-    for (size_t b = 0; b < boff.size(); b++) {
-        d->bdia_offsets[b] = boff[b];
-        d->bdia_bptr[b + 1] = d->bdia_bptr[b] + bcnt[b];
-    }
-    d->bdia_data = dia.dia_data;   // identical data layout
-    dia.dia_data = nullptr;
-    csp_free_dia_matrix(&dia);
-    return CSP_OK;
+    return bdia_from_dia(&dia, d);
 }
 
 // matrix_storage.h:1137 bdia2coo.

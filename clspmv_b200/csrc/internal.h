@@ -35,5 +35,9 @@ int device_count_dia(const int* row, const int* col, int nnz, int threshold, std
 int device_count_blocks(const int* rp, const int* col, int h, int nnz, const int* bh, const int* bw, const int* threshold,
                         int nshapes, std::vector<std::vector<BlockCounts>>& out);
 int ensure_sorted(coo_matrix_if* m);
+// The banding step of coo2bdia on a built DIA (consumed: its data moves into d).
+int bdia_from_dia(dia_matrix_iif* dia, bdia_matrix_iif* d);
+// true when a row-sorted COO holds two entries at one (row, col) position
+bool coo_has_duplicates(const coo_matrix_if* m);
 
 }  // namespace csp

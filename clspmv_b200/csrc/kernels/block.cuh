@@ -157,9 +157,9 @@ __global__ void __launch_bounds__(256) bcsr_generic_kernel(const int* __restrict
 // (fixed shuffle tree) and writes y.  Work item descriptor: {first block row,
 // block rows | blocks << 16, first block in the source (row-pointer) numbering, first
 // stored slot}.
-constexpr int kGbThreads = 256;
+constexpr int kGbThreads = 128;   // 8 CTAs per SM at 64 registers: their load and gather phases overlap
 constexpr int kGbBlocks = 4 * kGbThreads;
-constexpr int kGbRows = 256;
+constexpr int kGbRows = 128;
 
 // Row sums of one item: a lane group of G lanes per block row adds the row's block
 // products (prod, row order) and writes y = s_y + sum (s_y: the item's y rows).

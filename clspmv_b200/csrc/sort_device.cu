@@ -155,6 +155,8 @@ int bits_of(long long v)
     return b;
 }
 
+}  // namespace
+
 // Exclusive scan of a[0, n) on the device (chunk scans, then the chunk totals, recursively).
 int device_exclusive_scan(unsigned* a, size_t n, cudaStream_t st)
 {
@@ -173,40 +175,25 @@ int device_exclusive_scan(unsigned* a, size_t n, cudaStream_t st)
     return CSP_OK;
 }
 
-}  // namespace
 
-int device_sort_coo(coo_matrix_if* m)
+// Stable LSD radix sort of n 64-bit keys with 32-bit payloads over the low `bits` bits
+// of the keys; k0/v0 hold the input, k1/v1 are scratch of the same sizes; *kres/*vres
+// receive whichever pair of buffers holds the result.
+int device_radix_sort_pairs(uint64_t* k0, uint64_t* k1, unsigned* v0, unsigned* v1, long long n, int bits,
+                            cudaStream_t st, uint64_t** kres, unsigned** vres)
 {
-    const long long n = m->matinfo.nnz;
+    *kres = k0;
+    *vres = v0;
     if (n <= 1) return CSP_OK;
-    if (n > (long long)UINT32_MAX) return set_error(CSP_EUNSUP, "device sort: more than 2^32 entries");
-    const int cb = std::max(1, bits_of(std::max(m->matinfo.width, 1) - 1));
-    const int rb = std::max(1, bits_of(std::max(m->matinfo.height, 1) - 1));
-    const int passes = (rb + cb + 7) / 8;
+    const int passes = (std::max(bits, 1) + 7) / 8;
     const int ntiles = (int)((n + kSortTile - 1) / kSortTile);
-    DBuf drow, dcol, dval, dval2, k0, k1, v0, v1, hist;
-    SCUDA(cudaMalloc(&drow.p, n * 4));
-    SCUDA(cudaMalloc(&dcol.p, n * 4));
-    SCUDA(cudaMalloc(&dval.p, n * 4));
-    SCUDA(cudaMalloc(&dval2.p, n * 4));
-    SCUDA(cudaMalloc(&k0.p, n * 8));
-    SCUDA(cudaMalloc(&k1.p, n * 8));
-    SCUDA(cudaMalloc(&v0.p, n * 4));
-    SCUDA(cudaMalloc(&v1.p, n * 4));
+    DBuf hist;
     SCUDA(cudaMalloc(&hist.p, (size_t)256 * ntiles * sizeof(unsigned)));
-    cudaStream_t st = nullptr;
-    SCUDA(cudaMemcpy(drow.p, m->coo_row_id, n * 4, cudaMemcpyHostToDevice));
-    SCUDA(cudaMemcpy(dcol.p, m->coo_col_id, n * 4, cudaMemcpyHostToDevice));
-    SCUDA(cudaMemcpy(dval.p, m->coo_data, n * 4, cudaMemcpyHostToDevice));
-    const unsigned g = (unsigned)((n + 255) / 256);
-    pack_keys_kernel<<<g, 256, 0, st>>>(static_cast<int*>(drow.p), static_cast<int*>(dcol.p), n, cb,
-                                        static_cast<uint64_t*>(k0.p), static_cast<unsigned*>(v0.p));
-    SCUDA(cudaGetLastError());
-    uint64_t* kin = static_cast<uint64_t*>(k0.p);
-    uint64_t* kout = static_cast<uint64_t*>(k1.p);
-    unsigned* vin = static_cast<unsigned*>(v0.p);
-    unsigned* vout = static_cast<unsigned*>(v1.p);
     unsigned* hs = static_cast<unsigned*>(hist.p);
+    uint64_t* kin = k0;
+    uint64_t* kout = k1;
+    unsigned* vin = v0;
+    unsigned* vout = v1;
     for (int p = 0; p < passes; p++) {
         const int shift = 8 * p;
         radix_hist_kernel<<<ntiles, kSortThreads, 0, st>>>(kin, n, shift, ntiles, hs);
@@ -218,7 +205,42 @@ int device_sort_coo(coo_matrix_if* m)
         std::swap(kin, kout);
         std::swap(vin, vout);
     }
-    unpack_kernel<<<g, 256, 0, st>>>(kin, vin, static_cast<float*>(dval.p), n, cb, static_cast<int*>(drow.p),
+    *kres = kin;
+    *vres = vin;
+    return CSP_OK;
+}
+
+int device_sort_coo(coo_matrix_if* m)
+{
+    const long long n = m->matinfo.nnz;
+    if (n <= 1) return CSP_OK;
+    if (n > (long long)UINT32_MAX) return set_error(CSP_EUNSUP, "device sort: more than 2^32 entries");
+    const int cb = std::max(1, bits_of(std::max(m->matinfo.width, 1) - 1));
+    const int rb = std::max(1, bits_of(std::max(m->matinfo.height, 1) - 1));
+    DBuf drow, dcol, dval, dval2, k0, k1, v0, v1;
+    SCUDA(cudaMalloc(&drow.p, n * 4));
+    SCUDA(cudaMalloc(&dcol.p, n * 4));
+    SCUDA(cudaMalloc(&dval.p, n * 4));
+    SCUDA(cudaMalloc(&dval2.p, n * 4));
+    SCUDA(cudaMalloc(&k0.p, n * 8));
+    SCUDA(cudaMalloc(&k1.p, n * 8));
+    SCUDA(cudaMalloc(&v0.p, n * 4));
+    SCUDA(cudaMalloc(&v1.p, n * 4));
+    cudaStream_t st = nullptr;
+    SCUDA(cudaMemcpy(drow.p, m->coo_row_id, n * 4, cudaMemcpyHostToDevice));
+    SCUDA(cudaMemcpy(dcol.p, m->coo_col_id, n * 4, cudaMemcpyHostToDevice));
+    SCUDA(cudaMemcpy(dval.p, m->coo_data, n * 4, cudaMemcpyHostToDevice));
+    const unsigned g = (unsigned)((n + 255) / 256);
+    pack_keys_kernel<<<g, 256, 0, st>>>(static_cast<int*>(drow.p), static_cast<int*>(dcol.p), n, cb,
+                                        static_cast<uint64_t*>(k0.p), static_cast<unsigned*>(v0.p));
+    SCUDA(cudaGetLastError());
+    uint64_t* kres = nullptr;
+    unsigned* vres = nullptr;
+    int rc = device_radix_sort_pairs(static_cast<uint64_t*>(k0.p), static_cast<uint64_t*>(k1.p),
+                                     static_cast<unsigned*>(v0.p), static_cast<unsigned*>(v1.p), n, rb + cb, st, &kres,
+                                     &vres);
+    if (rc) return rc;
+    unpack_kernel<<<g, 256, 0, st>>>(kres, vres, static_cast<float*>(dval.p), n, cb, static_cast<int*>(drow.p),
                                      static_cast<int*>(dcol.p), static_cast<float*>(dval2.p));
     SCUDA(cudaGetLastError());
     SCUDA(cudaMemcpy(m->coo_row_id, drow.p, n * 4, cudaMemcpyDeviceToHost));

@@ -609,6 +609,19 @@ int csp_read_mmf_ex(const char* filename, coo_matrix_if* mat, int flags);
  * counterpart in the reference. */
 int csp_sort_coo_device(coo_matrix_if* mat);
 
+/* ------------------------------------------------------------------------ */
+/* Layout builds on the current CUDA device: the same structs, filled byte for */
+/* byte as by csp_coo2dia / csp_coo2bdia / csp_coo2bcsr (matrix_storage.h:937  */
+/* coo2dia, :1185 coo2bdia, :1595 coo2bcsr) when no two entries share a        */
+/* (row, col) position; with such                                              */
+/* duplicates the last one in input order is kept.  The same errors, at the    */
+/* same entry, as the host builds; CSP_ENODEV without a device.                */
+/* ------------------------------------------------------------------------ */
+int csp_coo2dia_device(coo_matrix_if* src, dia_matrix_iif* dst, int alignment);
+int csp_coo2bdia_device(coo_matrix_if* src, bdia_matrix_iif* dst, int alignment);     /* :1185 */
+int csp_coo2bcsr_device(coo_matrix_if* src, bcsr_matrix_if* dst, unsigned int bwidth, unsigned int bheight,
+                        int alignment);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif
