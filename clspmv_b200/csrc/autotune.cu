@@ -176,9 +176,61 @@ int build_sell_split(const Coo& a, int sh, double q, int csr_meth, cocktail_iif*
     return CSP_OK;
 }
 
+// Rows of at most t entries as a COO part (a segmented reduction gathering x from L2:
+// few entries, no partial sums to merge), longer rows whole as a CSR part with kernel
+// csr_meth (the x-panel one for random columns: its partial sums and merge then cover
+// only the long rows).
+int build_coo_split(const Coo& a, int t, int csr_meth, cocktail_iif* c)
+{
+    const coo_matrix_if* m = a.m;
+    const int h = m->matinfo.height;
+    std::vector<int> srow, scol, rrp((size_t)h + 1, 0), rcol;
+    std::vector<float> sval, rval;
+    for (int r = 0; r < h; r++) {
+        const bool shortrow = a.rp[r + 1] - a.rp[r] <= t;
+        for (int q = a.rp[r]; q < a.rp[r + 1]; q++) {
+            if (shortrow) {
+                srow.push_back(r);
+                scol.push_back(m->coo_col_id[q]);
+                sval.push_back(m->coo_data[q]);
+            } else {
+                rcol.push_back(m->coo_col_id[q]);
+                rval.push_back(m->coo_data[q]);
+            }
+        }
+        rrp[r + 1] = (int)rcol.size();
+    }
+    if (srow.empty() || rcol.empty()) return set_error(CSP_EFORMAT, "coo split: one side is empty");
+    coo_matrix_if& o = c->coo;
+    o.matinfo.width = m->matinfo.width;
+    o.matinfo.height = h;
+    o.matinfo.nnz = (int)srow.size();
+    o.coo_row_id = static_cast<int*>(malloc(srow.size() * sizeof(int)));
+    o.coo_col_id = static_cast<int*>(malloc(scol.size() * sizeof(int)));
+    o.coo_data = static_cast<float*>(malloc(sval.size() * sizeof(float)));
+    memcpy(o.coo_row_id, srow.data(), srow.size() * sizeof(int));
+    memcpy(o.coo_col_id, scol.data(), scol.size() * sizeof(int));
+    memcpy(o.coo_data, sval.data(), sval.size() * sizeof(float));
+    c->ifusecoo = true;
+    csr_matrix_if& e = c->csr;
+    e.matinfo.width = m->matinfo.width;
+    e.matinfo.height = h;
+    e.matinfo.nnz = (int)rcol.size();
+    e.csr_row_ptr = static_cast<int*>(malloc(rrp.size() * sizeof(int)));
+    e.csr_col_id = static_cast<int*>(malloc(rcol.size() * sizeof(int)));
+    e.csr_data = static_cast<float*>(malloc(rval.size() * sizeof(float)));
+    memcpy(e.csr_row_ptr, rrp.data(), rrp.size() * sizeof(int));
+    memcpy(e.csr_col_id, rcol.data(), rcol.size() * sizeof(int));
+    memcpy(e.csr_data, rval.data(), rval.size() * sizeof(float));
+    c->ifusecsr = true;
+    c->csr_meth_num = csr_meth;
+    return CSP_OK;
+}
+
 // Builds the candidate named `name` into c (fresh, zeroed).  Names: csr<m>, coo,
 // ell, sell<sh>, dia<m>, bdia<m>, bcsr<bh>x<bw>m<m>, bell<bh>x<bw>, sbell<bh>x<bw>,
-// ell<k>+csr<m>, sellq<sh>+csr<m> (m = the overflow CSR part's kernel), gbcsr<bh>x<bw>
+// ell<k>+csr<m>, sellq<sh>+csr<m> (m = the overflow CSR part's kernel), coo<t>+csr<m>
+// (rows of at most t entries as COO, the others as CSR), gbcsr<bh>x<bw>
 // (generic BCSR in the cocktail's bcsr member, CSP_METH_GENERIC_BCSR).  csr16 is the
 // x-panel kernel (CSP_METH_XPANEL).
 int build(const Coo& a, const std::string& name, cocktail_iif* c)
@@ -189,6 +241,7 @@ int build(const Coo& a, const std::string& name, cocktail_iif* c)
     int x = 0, y = 0, z = 0;
     if (sscanf(name.c_str(), "ell%d+csr%d", &x, &y) == 2) return build_ell_split(a, x, y, c);
     if (sscanf(name.c_str(), "sellq%d+csr%d", &x, &y) == 2) return build_sell_split(a, x, 0.75, y, c);
+    if (sscanf(name.c_str(), "coo%d+csr%d", &x, &y) == 2) return build_coo_split(a, x, y, c);
     if (sscanf(name.c_str(), "gbcsr%dx%d", &x, &y) == 2) {
         c->ifusebcsr = true;
         c->bcsr_meth_num = CSP_METH_GENERIC_BCSR;
@@ -321,6 +374,10 @@ std::vector<std::string> candidates(const Coo& a)
             if (k > 0 && k < a.maxlen) c.push_back("ell" + std::to_string(k) + tail);
             if (a.maxlen > 2 * mean + 1) c.push_back(std::string("sellq32") + tail);
         }
+        // short rows through COO, long rows whole through the x-panel kernel
+        if (a.maxlen > 64)
+            for (int t : {4, 8, 16})
+                if (t < a.maxlen) c.push_back("coo" + std::to_string(t) + "+csr16");
     }
     if (h == w && nnz > 0) {
         // DIA only if the padded storage stays within the reference's 2x rule: a failed

@@ -99,3 +99,20 @@ def test_cocktail_generic_bcsr_part(bs):
     assert np.isin(key, rows[ok].astype(np.int64) * w + cols[ok]).all()
     hd.free()
     mat.free()
+
+
+@pytest.mark.parametrize("choice", ["coo4+csr16", "coo8+csr16", "coo16+csr16", "coo8+csr2"])
+def test_coo_split_candidates(choice, tmp_path):
+    """The short-row split (rows of at most t entries as a COO part, the rest as a CSR
+    part with the x-panel or adaptive kernel), forced through the decision cache: the
+    first call records the pattern's key, the edited cache then names the candidate."""
+    case = CASES["zipf_100k"]
+    cache = str(tmp_path / "tune.txt")
+    analyze_matrix(coo_of(case), mode=CSP_ANALYZE_AUTOTUNE, cache_path=cache)
+    key = open(cache).read().split()[0]
+    with open(cache, "w") as f:
+        f.write(f"{key} {choice} 0.0\n")
+    mat = analyze_matrix(coo_of(case), mode=CSP_ANALYZE_AUTOTUNE, cache_path=cache)
+    assert mat.choice == choice
+    x, y0 = vecs(case[0], case[1])
+    check(case, run(mat, x, y0), x, y0)
