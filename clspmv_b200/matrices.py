@@ -144,19 +144,25 @@ def laplacian_sq(nx: int, ny: int):
 BATCH_KINDS = ("laplacian", "zipf", "block")
 
 
-def batch_mixed(count: int = 512, lo: int = 1_000, hi: int = 200_000, seed: int = 0):
+def batch_mixed(count: int = 512, lo: int = 1_000, hi: int = 200_000, seed: int = 0, first: int = 0,
+                n: int | None = None):
     """Uneven batch: `count` matrices with row counts log-uniform in [lo, hi], each
     drawn by seed from one of three generators at about 12 nonzeros per row --
     the squared Laplacian (laplacian_sq on a near-square grid), Zipf(1.85) row
     lengths clipped to [1, min(10000, n / 4)] (zipf_rows), or 3x3 blocks with block-row
-    degree uniform in [2, 6] (block_3x3, band +-2000 block columns).  Returns a list
-    of (kind, height, width, row, col, val)."""
+    degree uniform in [2, 6] (block_3x3, band +-2000 block columns).  Only matrices
+    [first, first + n) are built (a shard of the list; all of them by default): every
+    matrix's parameters are drawn in list order, so matrix i is the same in every shard
+    layout.  Returns a list of (kind, height, width, row, col, val)."""
     rng = np.random.default_rng(seed)
+    stop = count if n is None else min(count, first + n)
     out = []
-    for i in range(count):
+    for i in range(stop):
         rows = int(round(np.exp(rng.uniform(np.log(lo), np.log(hi)))))
         kind = BATCH_KINDS[int(rng.integers(0, 3))]
         s = int(rng.integers(0, 2**31 - 1))
+        if i < first:
+            continue
         if kind == "laplacian":
             nx = max(3, int(np.sqrt(rows)))
             ny = max(3, rows // nx)
@@ -166,3 +172,12 @@ def batch_mixed(count: int = 512, lo: int = 1_000, hi: int = 200_000, seed: int 
         else:
             out.append((kind,) + block_3x3(max(2, rows // 3), deg=(2, 6), band=2000, seed=s))
     return out
+
+
+def shard(total: int, world: int, rank: int) -> tuple[int, int]:
+    """(first, count) of rank's contiguous share of `total` independent units, the
+    first total % world ranks taking one more."""
+    if world < 1 or not 0 <= rank < world:
+        raise ValueError(f"rank {rank} of {world}")
+    base, extra = divmod(total, world)
+    return rank * base + min(rank, extra), base + (1 if rank < extra else 0)
