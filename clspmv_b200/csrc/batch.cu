@@ -137,21 +137,17 @@ void features(const HCsr& c, int flags, csp_batch_features& f)
         f.sell_slots[h] = slots;
     }
     // blocks
-    long long bcsr_long[3] = {0, 0, 0};   // most blocks in one block row
     for (int b = 2; b <= 4; b++) {
-        long long blocks = 0, longest = 0;
+        long long blocks = 0;
         std::vector<int> cols;
         for (int r0 = 0; r0 < m; r0 += b) {
             cols.clear();
             for (int r = r0; r < std::min(m, r0 + b); r++)
                 for (int j = c.rp[r]; j < c.rp[r + 1]; j++) cols.push_back(c.col[j] - c.col[j] % b);
             std::sort(cols.begin(), cols.end());
-            const long long nbk = std::unique(cols.begin(), cols.end()) - cols.begin();
-            blocks += nbk;
-            longest = std::max(longest, nbk);
+            blocks += std::unique(cols.begin(), cols.end()) - cols.begin();
         }
         f.bcsr_blocks[b - 2] = blocks;
-        bcsr_long[b - 2] = longest;
     }
     // candidates: CSR always; the padded formats while they store at most 1.5x the entries
     // (sliced ELL: 2x, since its per-row lane needs no reduction and short, even rows --
@@ -162,10 +158,8 @@ void features(const HCsr& c, int flags, csp_batch_features& f)
         if (f.sell_slots[0] <= sell_lim && f.sell_slots[0] < INT_MAX) feas |= 1u << CSP_BFMT_SELL32;
         if (f.sell_slots[1] <= sell_lim && f.sell_slots[1] < INT_MAX) feas |= 1u << CSP_BFMT_SELL128;
         if (dia_ok && (double)offs.size() * m <= lim && f.dia_slots < INT_MAX) feas |= 1u << CSP_BFMT_DIA;
-        // BCSR also needs every block row to fit one warp item (rounded start included)
         for (int b = 2; b <= 4; b++)
-            if ((double)f.bcsr_blocks[b - 2] * b * b <= lim && f.bcsr_blocks[b - 2] * b * b < INT_MAX &&
-                bcsr_long[b - 2] + dev::kBcsrNb(b) - 1 <= dev::kBcsrSlots(b))
+            if ((double)f.bcsr_blocks[b - 2] * b * b <= lim && f.bcsr_blocks[b - 2] * b * b < INT_MAX)
                 feas |= 1u << (CSP_BFMT_BCSR2 + b - 2);
     }
     f.feasible = feas;
@@ -403,22 +397,12 @@ void build_bcsr(const HCsr& c, int B, HPart& p)
             p.v[(size_t)q * al + blk] += c.val[j];
         }
     }
-    // block columns padded to whole groups of 4: the kernel loads a lane's column ids
-    // with one vector load
-    p.i1.resize((size_t)al, 0);
-    // items: runs of whole block rows whose blocks fit one warp (kBcsrSlots block slots
-    // from the first block rounded down to kBcsrNb, at most kBcsrRows block rows); the
-    // format is feasible only when every block row fits by itself
-    const int NB = dev::kBcsrNb(B), cap = dev::kBcsrSlots(B), rcap = dev::kBcsrRows(B);
-    p.ranges.clear();
-    for (int br = 0; br < nbr;) {
-        const int ba = p.i0[br] & ~(NB - 1);
-        int e = br;
-        while (e < nbr && e - br < rcap && p.i0[e + 1] - ba <= cap) e++;
-        if (e == br) e = br + 1;   // not reached: the format is feasible only when every block row fits
-        p.ranges.push_back(range_item(0, 0, make_int4(br, e - br, p.i0[br], p.i0[e])));
-        br = e;
-    }
+    const int brpv = dev::kBatchBcsrRows;   // block rows per virtual block
+    const int nvb = (nbr + brpv - 1) / brpv;
+    std::vector<long long> vs((size_t)nvb);
+    for (int vb = 0; vb < nvb; vb++)
+        vs[vb] = (long long)B * B * (p.i0[std::min(nbr, (vb + 1) * brpv)] - p.i0[vb * brpv]);
+    cut_items(p, nvb, vs);
 }
 
 void build_part(int fmt, const HCsr& c, HPart& p)

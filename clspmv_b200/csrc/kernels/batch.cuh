@@ -40,14 +40,8 @@ constexpr int kWarpNnz = 32 * 4 * kWarpVecs - 4; // CSR item entries (room for t
 constexpr int kWarpRows = 64;                    // CSR item rows
 constexpr int kBatchDiaRows = 4 * 32;            // DIA step: four consecutive rows per lane
 constexpr int kBatchSellRows = 32;               // SELL step: a row per lane
-// BCSR items: each lane holds kBcsrNb(B) consecutive blocks (4, 2, 1 for B = 2, 3, 4:
-// as many as 64 registers hold without spilling), an item at most
-// kBcsrSlots(B) block slots (from its first block rounded down to kBcsrNb) and
-// kWarpRows / B block rows, so that its products (B per block) and y rows fit the
-// warp's shared memory
-__host__ __device__ constexpr int kBcsrNb(int B) { return B <= 2 ? 4 : B == 3 ? 2 : 1; }
-__host__ __device__ constexpr int kBcsrSlots(int B) { return 32 * kBcsrNb(B) < 256 / B ? 32 * kBcsrNb(B) : 256 / B; }
-__host__ __device__ constexpr int kBcsrRows(int B) { return 64 / B; }
+constexpr int kBatchBcsrLanes = 2;               // BCSR: lanes per block row
+constexpr int kBatchBcsrRows = 32 / kBatchBcsrLanes;   // BCSR step: block rows per warp
 constexpr int kBatchReserve = 4;                 // items a warp takes from the counter at once
 
 struct BatchPart {
@@ -313,155 +307,69 @@ __device__ __forceinline__ void batch_dia(const BatchPart& P, int vb, int lane)
         if (r0 + q < m) P.y[r0 + q] = yo[q] + acc[q];
 }
 
-template <class V, int NB> struct Planes;
-template <class V> struct Planes<V, 4> {
-    __device__ __forceinline__ static float4 ld(const V* p) { return Val<V>::ld4(p); }
-};
-template <> struct Planes<float, 2> {
-    __device__ __forceinline__ static float4 ld(const float* p)
-    {
-        const float2 v = __ldg(reinterpret_cast<const float2*>(p));
-        return make_float4(v.x, v.y, 0.0f, 0.0f);
-    }
-};
-template <class V> struct Planes<V, 1> {
-    __device__ __forceinline__ static float4 ld(const V* p) { return make_float4(Val<V>::ld(p), 0.0f, 0.0f, 0.0f); }
-};
-template <> struct Planes<__nv_bfloat16, 2> {
-    __device__ __forceinline__ static float4 ld(const __nv_bfloat16* p)
-    {
-        const unsigned u = __ldg(reinterpret_cast<const unsigned*>(p));
-        return make_float4(__uint_as_float(u << 16), __uint_as_float(u & 0xffff0000u), 0.0f, 0.0f);
-    }
-};
-__device__ __forceinline__ float f4(const float4& v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
-
-// Row sums of a BCSR item: a lane group of G lanes per block row adds the B products of
-// each of its blocks (ws.prod, B floats per block slot, in block order) and writes the
-// block row's y rows; with the gradient each block slot learns its block row.
-template <int B, int G, bool GRAD>
-__device__ __forceinline__ void bcsr_rows(WarpSmem& ws, int br0, int nrows, int m, float* __restrict__ y, int lane)
-{
-    const float* prod = reinterpret_cast<const float*>(ws.prod);
-    const int sub = lane % G;
-    constexpr int ngroups = 32 / G;
-    for (int first = 0; first < nrows; first += ngroups) {
-        const int lr = first + lane / G;
-        const bool valid = lr < nrows;
-        const int a = valid ? ws.rp[lr] : 0, b = valid ? ws.rp[lr + 1] : 0;
-        float acc[B];
-#pragma unroll
-        for (int h = 0; h < B; h++) acc[h] = 0.0f;
-        for (int k = a + sub; k < b; k += G) {
-#pragma unroll
-            for (int h = 0; h < B; h++) acc[h] += prod[k * B + h];
-            if (GRAD) ws.rowid[k] = (unsigned char)lr;
-        }
-#pragma unroll
-        for (int h = 0; h < B; h++) {
-            const float t = group_sum<G>(acc[h]);
-            const int r = (br0 + lr) * B + h;
-            if (valid && sub == 0 && r < m) y[r] = ws.ys[lr * B + h] + t;
-        }
-    }
-}
-
-// BCSR work block: block rows [br0, br0 + nrows) whose blocks [b0, b1) fit the warp.
-// Lane l holds the NB consecutive block slots from ba + NB * l (ba = b0 rounded down to
-// NB): one load of NB column ids and one of NB values per element plane, so every
-// matrix byte moves in a coalesced load of NB elements, and all its x gathers are in
-// flight together.  Each block's B row products go to the warp's shared memory, a lane
-// group per block row adds them in block order, and the gradient of each element plane
-// is one store of NB values.
+// BCSR block rows [vb * 16, vb * 16 + 16): kBatchBcsrLanes (2) lanes per block row,
+// each lane taking two of its row's blocks per round, whose column ids, values and x
+// gathers are all requested before any is used (the batch's block rows hold a few
+// blocks each: one or two rounds).
 template <class V, int B, bool GRAD>
-__device__ __forceinline__ void batch_bcsr(WarpSmem& ws, const BatchPart& P, const BatchItem& it, int lane)
+__device__ __forceinline__ void batch_bcsr(const BatchPart& P, int vb, int lane32)
 {
-    constexpr int NB = kBcsrNb(B);
-    const int br0 = it.blk.x, nrows = it.blk.y, b0 = it.blk.z, b1 = it.blk.w;
-    const int ba = b0 & ~(NB - 1);
-    if (b1 - ba > kBcsrSlots(B) || nrows > kBcsrRows(B)) return;   // the host builds no such item
-    const int j = ba + NB * lane;
-    const int m = P.m, n = P.n;
-    const size_t al = (size_t)P.stride;
+    constexpr int G = kBatchBcsrLanes;
+    constexpr int U = B <= 3 ? 2 : 1;   // two 4x4 blocks in registers would spill
+    const int br = vb * kBatchBcsrRows + lane32 / G, lane = lane32 % G;
+    const bool valid = br < P.nbr;
+    const int s = valid ? __ldg(P.i0 + br) : 0, e = valid ? __ldg(P.i0 + br + 1) : 0;
     const V* __restrict__ data = static_cast<const V*>(P.v);
-    const bool act = j < b1;
-    int cc[NB];
-    float4 a[B * B];
+    const float* __restrict__ x = P.x;
+    const size_t al = (size_t)P.stride;
+    const int m = P.m, n = P.n;
+    float yb[B];
+    if (GRAD) {
 #pragma unroll
-    for (int k = 0; k < NB; k++) cc[k] = 0;
+        for (int h = 0; h < B; h++) yb[h] = (valid && br * B + h < m) ? __ldg(P.ybar + br * B + h) : 0.0f;
+    }
+    // the block row's y, requested with its first blocks, not after the last
+    float yo[B];
 #pragma unroll
-    for (int q = 0; q < B * B; q++) a[q] = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (act) {
-        if (NB == 4) {
-            const int4 c4 = ld_int4(P.i1 + j);
-            cc[0] = c4.x; cc[1 % NB] = c4.y; cc[2 % NB] = c4.z; cc[3 % NB] = c4.w;
-        } else if (NB == 2) {
-            const int2 c2 = __ldg(reinterpret_cast<const int2*>(P.i1 + j));
-            cc[0] = c2.x; cc[1 % NB] = c2.y;
-        } else {
-            cc[0] = __ldg(P.i1 + j);
+    for (int h = 0; h < B; h++) yo[h] = (valid && lane == 0 && br * B + h < m) ? P.y[br * B + h] : 0.0f;
+    float acc[B];
+#pragma unroll
+    for (int h = 0; h < B; h++) acc[h] = 0.0f;
+    for (int j0 = s + lane; j0 < e; j0 += G * U) {
+        int c0[U];
+        float a[U][B * B];
+        float xv[U][B];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int j = j0 + u * G;
+            const bool in = j < e;
+            c0[u] = in ? __ldg(P.i1 + j) : 0;
+#pragma unroll
+            for (int q = 0; q < B * B; q++) a[u][q] = in ? Val<V>::ld(data + (size_t)q * al + j) : 0.0f;
         }
 #pragma unroll
-        for (int q = 0; q < B * B; q++) a[q] = Planes<V, NB>::ld(data + (size_t)q * al + j);
-    }
-    // the item's block-row pointers and y rows, requested with the blocks
-    for (int i = lane; i <= nrows; i += 32) ws.rp[i] = (i < nrows ? __ldg(P.i0 + br0 + i) : b1) - ba;
-    for (int i = lane; i < nrows * B; i += 32) ws.ys[i] = br0 * B + i < m ? P.y[br0 * B + i] : 0.0f;
-    float xv[NB][B];
+        for (int u = 0; u < U; u++)
 #pragma unroll
-    for (int k = 0; k < NB; k++) {
-        const bool in = j + k >= b0 && j + k < b1;
+            for (int w = 0; w < B; w++) xv[u][w] = (j0 + u * G < e && c0[u] + w < n) ? ldx(x, c0[u] + w) : 0.0f;
 #pragma unroll
-        for (int w = 0; w < B; w++) xv[k][w] = (in && cc[k] + w < n) ? ldx(P.x, cc[k] + w) : 0.0f;
-    }
-    float* prod = reinterpret_cast<float*>(ws.prod);
+        for (int u = 0; u < U; u++) {
 #pragma unroll
-    for (int k = 0; k < NB; k++) {
-        if (j + k < b0 || j + k >= b1) continue;
+            for (int h = 0; h < B; h++)
 #pragma unroll
-        for (int h = 0; h < B; h++) {
-            float t = 0.0f;
+                for (int w = 0; w < B; w++) acc[h] += a[u][h * B + w] * xv[u][w];
+            if (GRAD && j0 + u * G < e) {
 #pragma unroll
-            for (int w = 0; w < B; w++) t += f4(a[h * B + w], k) * xv[k][w];
-            prod[(j + k - ba) * B + h] = t;
-        }
-    }
-    __syncwarp();
-    if (nrows <= 1) bcsr_rows<B, 32, GRAD>(ws, br0, nrows, m, P.y, lane);
-    else if (nrows <= 2) bcsr_rows<B, 16, GRAD>(ws, br0, nrows, m, P.y, lane);
-    else if (nrows <= 4) bcsr_rows<B, 8, GRAD>(ws, br0, nrows, m, P.y, lane);
-    else if (nrows <= 8) bcsr_rows<B, 4, GRAD>(ws, br0, nrows, m, P.y, lane);
-    else if (nrows <= 16) bcsr_rows<B, 2, GRAD>(ws, br0, nrows, m, P.y, lane);
-    else bcsr_rows<B, 1, GRAD>(ws, br0, nrows, m, P.y, lane);
-    if (GRAD) __syncwarp();   // every lane: the block rows in ws.rowid are complete
-    if (GRAD && act) {
-        float yb[NB][B];
+                for (int h = 0; h < B; h++)
 #pragma unroll
-        for (int k = 0; k < NB; k++) {
-            const bool in = j + k >= b0 && j + k < b1;
-            const int lr = in ? ws.rowid[j + k - ba] : 0;
-#pragma unroll
-            for (int h = 0; h < B; h++) {
-                const int r = (br0 + lr) * B + h;
-                yb[k][h] = (in && r < m) ? __ldg(P.ybar + r) : 0.0f;
+                    for (int w = 0; w < B; w++) P.abar[(size_t)(h * B + w) * al + j0 + u * G] = yb[h] * xv[u][w];
             }
         }
+    }
 #pragma unroll
-        for (int q = 0; q < B * B; q++) {
-            float g[NB];
-#pragma unroll
-            for (int k = 0; k < NB; k++) g[k] = yb[k][q / B] * xv[k][q % B];
-            float* dst = P.abar + (size_t)q * al + j;
-            if (j >= b0 && j + NB <= b1) {
-                if (NB == 4) __stcs(reinterpret_cast<float4*>(dst), make_float4(g[0], g[1 % NB], g[2 % NB], g[3 % NB]));
-                else if (NB == 2) __stcs(reinterpret_cast<float2*>(dst), make_float2(g[0], g[1 % NB]));
-                else __stcs(dst, g[0]);
-            } else {
-#pragma unroll
-                for (int k = 0; k < NB; k++)
-                    if (j + k >= b0 && j + k < b1) dst[k] = g[k];
-            }
-        }
+    for (int h = 0; h < B; h++) {
+        const float t = group_sum<G>(acc[h]);
+        const int r = br * B + h;
+        if (valid && lane == 0 && r < m) P.y[r] = yo[h] + t;
     }
 }
 
@@ -476,9 +384,15 @@ __device__ __forceinline__ void batch_item(WarpSmem& ws, const BatchPart& P, con
     case BK_DIA:
         for (int vb = it.v0; vb < it.v1; vb++) batch_dia<V, GRAD>(P, vb, lane);
         break;
-    case BK_BCSR2: batch_bcsr<V, 2, GRAD>(ws, P, it, lane); break;
-    case BK_BCSR3: batch_bcsr<V, 3, GRAD>(ws, P, it, lane); break;
-    case BK_BCSR4: batch_bcsr<V, 4, GRAD>(ws, P, it, lane); break;
+    case BK_BCSR2:
+        for (int vb = it.v0; vb < it.v1; vb++) batch_bcsr<V, 2, GRAD>(P, vb, lane);
+        break;
+    case BK_BCSR3:
+        for (int vb = it.v0; vb < it.v1; vb++) batch_bcsr<V, 3, GRAD>(P, vb, lane);
+        break;
+    case BK_BCSR4:
+        for (int vb = it.v0; vb < it.v1; vb++) batch_bcsr<V, 4, GRAD>(P, vb, lane);
+        break;
     }
 }
 

@@ -17,11 +17,6 @@ CASES.update(duplicate_cases())
 CASES["lap_sq"] = M.laplacian_sq(30, 21)
 CASES["block"] = M.block_3x3(300, deg=(2, 6), band=50, seed=4)
 CASES["zipf"] = M.zipf_rows(3000, s=1.85, max_len=700, seed=4)
-# dense 12 x 480: full blocks, but one block row of 240 / 160 / 120 blocks is longer than a
-# batch item holds, so no BCSR format is feasible
-_d = np.argwhere(np.ones((12, 480), bool))
-CASES["wide_dense"] = (12, 480, _d[:, 0].astype(np.int32), _d[:, 1].astype(np.int32),
-                       np.ones(_d.shape[0], np.float32))
 
 
 def _expected(case, bf16=False):
@@ -38,11 +33,10 @@ def _expected(case, bf16=False):
         pad[:h] = lens
         sell.append(int(pad.reshape(-1, H).max(axis=1).sum() * H) if h else 0)
     f["sell_slots"] = sell
-    blocks, longest = [], []
+    blocks = []
     for b in (2, 3, 4):
         key = np.unique((r.astype(np.int64) // b) * (w + b) + (c - c % b))
         blocks.append(int(key.size))
-        longest.append(int(np.bincount(key // (w + b)).max()) if key.size else 0)
     f["bcsr_blocks"] = blocks
     lim, sell_lim = 1.5 * nnz + 64, 2.0 * nnz + 64
     feas = 1 << CSP_BFMT_CSR
@@ -54,10 +48,7 @@ def _expected(case, bf16=False):
         if ndiag >= 0 and ndiag * h <= lim:
             feas |= 1 << CSP_BFMT_DIA
         for b in (2, 3, 4):
-            # every block row must fit one warp item: 128 / 64 / 32 block slots for
-            # 4 / 2 / 1 blocks per lane, less the rounding of its first block
-            nb, slots = {2: (4, 128), 3: (2, 64), 4: (1, 32)}[b]
-            if blocks[b - 2] * b * b <= lim and longest[b - 2] + nb - 1 <= slots:
+            if blocks[b - 2] * b * b <= lim:
                 feas |= 1 << (CSP_BFMT_BCSR2 + b - 2)
     f["feasible"] = feas
     es = 2.0 if bf16 else 4.0
@@ -109,9 +100,3 @@ def test_create_without_device():
     with pytest.raises(CspError) as e:
         Batch([COO(*CASES["lap_sq"])])
     assert e.value.code == CSP_ENODEV
-
-
-def test_long_block_rows_rule_out_bcsr():
-    f = features(COO(*CASES["wide_dense"]))
-    for b in (2, 3, 4):
-        assert not f["feasible"] & (1 << (CSP_BFMT_BCSR2 + b - 2)), b
