@@ -57,6 +57,32 @@ def test_device_calls_fail_cleanly_without_gpu(L):
     assert not h.value
 
 
+def test_device_setup_calls_refuse_without_gpu(L):
+    """The device sort and the device layout builds check for a device before any work:
+    CSP_ENODEV, and the input COO (which the builds may sort in place) unchanged."""
+    import torch
+    if torch.cuda.is_available():
+        return
+    from tests.fmt_extract import extract
+    r = np.array([2, 0, 1], np.int32)
+    c = np.array([1, 0, 2], np.int32)
+    v = np.array([3.0, 1.0, 2.0], np.float32)
+    for fn, st, args in (("csp_sort_coo_device", None, ()), ("csp_coo2dia_device", capi.dia_matrix, (32,)),
+                         ("csp_coo2bdia_device", capi.bdia_matrix, (32,)),
+                         ("csp_coo2bcsr_device", capi.bcsr_matrix, (3, 3, 32))):
+        coo = COO(3, 3, r.copy(), c.copy(), v.copy())
+        before = extract("coo", coo.s)
+        call = getattr(L, fn)
+        if st is None:
+            rc = call(coo.ref())
+        else:
+            out = st()
+            rc = call(coo.ref(), C.byref(out), *args)
+        assert rc == capi.CSP_ENODEV, (fn, rc)
+        after = extract("coo", coo.s)
+        assert all(np.array_equal(np.asarray(before[k]), np.asarray(after[k])) for k in ("row", "col", "val")), fn
+
+
 def test_temporary_coo_outlives_the_call(L):
     """`COO(...).ref()` passed straight to a conversion: the struct keeps the arrays its
     pointers reference alive through the call (large arrays, whose memory would
